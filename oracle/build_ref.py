@@ -1,0 +1,155 @@
+#!/usr/bin/env python3
+"""Build recipe for oracle/_ref: the reference's own CPU verification loops.
+
+TEST INFRASTRUCTURE ONLY.  Run in a container where the reference checkout
+is present (default /root/reference, or $OTS_REFERENCE_DIR).  For each pinned
+stencil it copies the CPU loop of the reference runner -- the lines between
+``memcpy(refB, hostData, arraySize);`` and ``memcpy(reference, refA,
+arraySize);`` of its main() -- verbatim into ``oracle/_ref/<name>_loop.inc``
+(git-ignored; nothing from the reference is committed), then compiles
+``oracle/ref_harness.cpp`` around those loops with the reference's own flags
+(``g++ -O2``, config.ninja:4) into ``oracle/_ref/libots_ref.so``.
+
+The built library is the "reference" CPU baseline and the generator of the
+golden vectors in tests/golden/.  When the reference tree is absent (e.g. on
+a machine that only received the prebuilt library) this script does nothing.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT = os.path.join(HERE, "_ref")
+
+# name -> reference runner source, relative to the reference root
+LOOPS = {
+    "jacobi_1d": "opencl/jacobi-1d/jacobi-1d.cpp",
+    "jacobi_1d_5pt": "opencl/jacobi-1d-5pt/jacobi-1d-5pt.cpp",
+    "jacobi_1d_7pt": "opencl/jacobi-1d-7pt/jacobi-1d-7pt.cpp",
+    "jacobi_2d": "opencl/jacobi-2d/jacobi-2d.cpp",
+    "poisson_2d": "opencl/poisson-2d/poisson-2d.cpp",
+    "gradient_2d": "opencl/gradient-2d/gradient-2d.cpp",
+}
+# jacobi-3d's loop (opencl/jacobi-3d/jacobi-3d.cpp:726-747) is deliberately
+# not built: its unparenthesised ARRAY_REF macro reads out of bounds.
+
+# name -> runner whose input fill loop is enabled (not under #if 0)
+FILLS = {
+    "fill_poisson_2d": ("opencl/poisson-2d/poisson-2d.cpp", 2, ["hostData"]),
+    "fill_fdtd_2d": ("opencl/fdtd-2d/fdtd-2d.cpp", 2, ["hostDataEX", "hostDataEY", "hostDataHZ"]),
+    "fill_cs_3d": ("opencl/cs-3d/cs-3d.cpp", 3, ["hostData"]),
+    "fill_jacobi_1d_5pt": ("opencl/jacobi-1d-5pt/jacobi-1d-5pt.cpp", 1, ["hostData"]),
+}
+
+# name -> (runner source, dims, has blockSizeY/Z members)
+GEOMETRY = {
+    "jacobi_1d": ("opencl/jacobi-1d/jacobi-1d.cpp", 1),
+    "jacobi_1d_5pt": ("opencl/jacobi-1d-5pt/jacobi-1d-5pt.cpp", 1),
+    "jacobi_1d_7pt": ("opencl/jacobi-1d-7pt/jacobi-1d-7pt.cpp", 1),
+    "jacobi_2d": ("opencl/jacobi-2d/jacobi-2d.cpp", 2),
+    "jacobi_3d": ("opencl/jacobi-3d/jacobi-3d.cpp", 3),
+    "poisson_2d": ("opencl/poisson-2d/poisson-2d.cpp", 2),
+    "poisson_3d": ("opencl/poisson-3d/poisson-3d.cpp", 3),
+    "gradient_2d": ("opencl/gradient-2d/gradient-2d.cpp", 2),
+    "gradient_3d": ("opencl/gradient-3d/gradient-3d.cpp", 3),
+    "fdtd_2d": ("opencl/fdtd-2d/fdtd-2d.cpp", 2),
+    "rician_denoise_2d": ("opencl/rician-denoise-2d/rician-denoise-2d.cpp", 2),
+    "cdsc_tv_update_2d": ("opencl/cdsc-tv-update-2d/cdsc-tv-update-2d.cpp", 2),
+    "cs_3d": ("opencl/cs-3d/cs-3d.cpp", 3),
+}
+
+START = "memcpy(refB, hostData, arraySize);"
+END = "memcpy(reference, refA, arraySize);"
+
+
+def extract(ref_root, rel):
+    path = os.path.join(ref_root, rel)
+    with open(path) as fh:
+        lines = fh.readlines()
+    s = next(i for i, l in enumerate(lines) if l.strip() == START)
+    e = next(i for i, l in enumerate(lines) if i > s and l.strip() == END)
+    body = lines[s + 1:e]
+    if not any("for(int t = 0; t < params.timeSteps; ++t)" in l for l in body):
+        raise RuntimeError("%s: CPU loop not found between the markers" % rel)
+    # 1-based line number of the first copied line, for diagnostics
+    return s + 2, "".join(body), path
+
+
+def extract_between(path, start_pred, end_pred):
+    with open(path) as fh:
+        lines = fh.readlines()
+    s = next(i for i, l in enumerate(lines) if start_pred(l))
+    e = next(i for i, l in enumerate(lines) if i > s and end_pred(l))
+    return s + 1, "".join(lines[s:e + 1])
+
+
+def gen_geometry_and_fill(ref_root):
+    """Generate oracle/_ref/ref_gen.cpp: each runner's GeneratorParams struct
+    (copied verbatim into its own namespace) behind a C entry point, and the
+    enabled input-fill loops behind C entry points.  boost::math::gcd/lcm are
+    supplied by oracle/ref_shim.hpp."""
+    out = ['#include "ref_shim.hpp"\n']
+    for name, (rel, dims) in GEOMETRY.items():
+        path = os.path.join(ref_root, rel)
+        line, body = extract_between(path, lambda l: l.startswith("struct GeneratorParams"),
+                                     lambda l: l.startswith("};"))
+        out.append("namespace geo_%s {\n#line %d \"%s\"\n%s\n}\n" % (name, line, path, body))
+        sets = ["p.problemSize = n;", "p.timeTileSize = T;", "p.blockSizeX = bx;",
+                "p.elementsPerThread = E;"]
+        gets = ["o[0] = p.padding;", "o[1] = p.paddedSize;", "o[2] = p.realSize;",
+                "o[3] = p.sizeLCM;", "o[4] = p.compsPerBlockX;", "o[7] = p.realPerBlockX;",
+                "o[10] = p.numBlocksX;", "o[13] = p.sharedSizeX;"]
+        if dims >= 2:
+            sets += ["p.blockSizeY = by;"]
+            gets += ["o[5] = p.compsPerBlockY;", "o[8] = p.realPerBlockY;",
+                     "o[11] = p.numBlocksY;", "o[14] = p.sharedSizeY;"]
+        if dims >= 3:
+            sets += ["p.blockSizeZ = bz;"]
+            gets += ["o[6] = p.compsPerBlockZ;", "o[9] = p.realPerBlockZ;",
+                     "o[12] = p.numBlocksZ;", "o[15] = p.sharedSizeZ;"]
+        out.append(
+            'extern "C" int ref_geometry_%s(int n, int T, int bx, int by, int bz, int E, int* o) {\n'
+            "  (void)by; (void)bz;\n"
+            "  for (int i = 0; i < 16; ++i) o[i] = 0;\n"
+            "  try {\n    geo_%s::GeneratorParams p;\n    %s\n    p.computeDerived();\n    %s\n"
+            "  } catch (...) { return -1; }\n  return 0;\n}\n"
+            % (name, name, " ".join(sets), " ".join(gets)))
+    for name, (rel, dims, arrays) in FILLS.items():
+        path = os.path.join(ref_root, rel)
+        line, body = extract_between(path, lambda l: l.strip() == "// Fill host arrays",
+                                     lambda l: l.strip() == "// Compute reference")
+        args = ", ".join("float* %s" % a for a in arrays)
+        out.append(
+            'extern "C" void ref_%s(%s, int paddedSize, int padding, unsigned seed) {\n'
+            "  RefParams params; params.paddedSize = paddedSize; params.padding = padding;\n"
+            "  params.timeSteps = 0;\n  srand(seed);\n#line %d \"%s\"\n%s\n}\n"
+            % (name, args, line, path, body))
+    with open(os.path.join(OUT, "ref_gen.cpp"), "w") as fh:
+        fh.write("".join(out))
+
+
+def build(ref_root=None, cxx="g++", verbose=False):
+    ref_root = ref_root or os.environ.get("OTS_REFERENCE_DIR", "/root/reference")
+    if not os.path.isdir(os.path.join(ref_root, "opencl")):
+        if verbose:
+            print("build_ref: reference tree not present; keeping prebuilt oracle/_ref")
+        return False
+    os.makedirs(OUT, exist_ok=True)
+    for name, rel in LOOPS.items():
+        line, body, path = extract(ref_root, rel)
+        with open(os.path.join(OUT, name + "_loop.inc"), "w") as fh:
+            fh.write('#line %d "%s"\n' % (line, path))
+            fh.write(body)
+    gen_geometry_and_fill(ref_root)
+    lib = os.path.join(OUT, "libots_ref.so")
+    cmd = [cxx, "-O2", "-g", "-fPIC", "-shared", "-I", OUT, "-I", HERE,
+           os.path.join(HERE, "ref_harness.cpp"), os.path.join(OUT, "ref_gen.cpp"), "-o", lib]
+    subprocess.check_call(cmd)
+    if verbose:
+        print("build_ref: built", lib)
+    return True
+
+
+if __name__ == "__main__":
+    ok = build(sys.argv[1] if len(sys.argv) > 1 else None, verbose=True)
+    sys.exit(0)
