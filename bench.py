@@ -1,0 +1,377 @@
+#!/usr/bin/env python3
+"""Benchmark: FP32 Jacobi-3D 7-point, 512^3 interior, 100 time steps.
+
+One "step" of this bench is one full run of the workload (100 time steps over
+the 512^3 grid, ceil(100/T) kernel launches).  Reported metric: grid-point
+updates per second (GUpdates/s = 512^3 * 100 / time), whole job over all
+ranks.
+
+  value    device time (CUDA events on the plan's stream) with the input
+           resident in HBM; the z-streamed time-tiled kernel with the
+           exhaustive-sweep-tuned (T, block, E) from tuned.json.
+  e2e      the same metric through the public C ABI with host buffers:
+           each step uploads the padded 520^3 host array from pinned memory
+           (ots_upload), runs, and downloads the result (ots_download).
+  plain    the plain one-step-per-launch kernel, same device timing (the
+           comparator of the >= 2x target), reported under "plain".
+  roofline HBM: algorithmic bytes per launch (read + write each cell once,
+           8 B x 512^3) / average launch time, against the measured copy
+           bandwidth in MEASURED_PEAKS.json.
+  cpu_baseline  the CPU oracle (a C restatement of the reference's per-point
+           arithmetic) on a bounded sample of the same grid, one core.
+
+Inputs (2 x 537 MB) are larger than the 126 MB L2, so no flush is needed.
+
+--impl reference times the reference's CPU path (the oracle restatement;
+the reference's own jacobi-3d CPU check indexes out of bounds and cannot
+run) on all host cores, on a bounded sample of the same workload.
+
+Multi-GPU: replicas only (the reference is single-device): each rank runs
+its own 512^3 problem on its own GPU; the timed region is bracketed by
+barriers and the time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "ics-12-overlapped-tiling_b200"))
+
+N, STEPS = 512, 100
+STENCIL = "jacobi-3d"
+BYTES_PER_UPDATE = 8.0       # read + write each cell once per launch (T=1 equivalent)
+FLOPS_PER_UPDATE = 7.0       # reference constant, opencl/jacobi-3d/jacobi-3d.cpp:915-917
+DEFAULT_CFG = dict(kernel="stream", T=4, bx=32, by=8, bz=1, E=4)
+
+
+def tuned_config():
+    path = os.path.join(ROOT, "ics-12-overlapped-tiling_b200", "ots", "tuned.json")
+    try:
+        with open(path) as fh:
+            cfg = json.load(fh)["jacobi-3d/512/100"]
+        return dict(kernel=cfg["kernel"], T=cfg["T"], bx=cfg["bx"], by=cfg["by"], bz=cfg.get("bz", 1),
+                    E=cfg["E"]), "exhaustive-sweep best (tuned.json)"
+    except Exception:
+        return dict(DEFAULT_CFG), "default"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            m = json.load(fh)
+        return float(m["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic(kernel):
+    """DRAM bytes per launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as fh:
+            t = json.load(fh)
+        e = t.get("%s/%s" % (STENCIL, kernel))
+        return None if e is None else float(e["bytes_per_launch_full"])
+    except Exception:
+        return None
+
+
+class Clocks:
+    """Samples nvidia-smi during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join("/tmp", "ots_clocks_%d.csv" % os.getpid())
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        try:
+            self.fh.close()
+        except Exception:
+            pass
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 7:
+                    rows.append(parts)
+        except Exception:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = sorted(float(r[0]) for r in rows if r[0].replace(".", "").isdigit())
+        mx = max(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[3 + i] == "Active"})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def reduce_max(t, world):
+    if world == 1:
+        return t
+    import torch
+    import torch.distributed as dist
+    x = torch.tensor([t], dtype=torch.float64, device="cuda")
+    dist.all_reduce(x, op=dist.ReduceOp.MAX)
+    return float(x.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_sample(threads, target_s):
+    """Time the CPU oracle on 512^3 with as many steps as fit ~target_s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle as O  # the checker, used here only as the CPU baseline
+    O.set_threads(threads)
+    pad = 1
+    P = N + 2 * pad
+    x = O.fill_ref(3, P, pad, P - pad, 123456, 1)[0]
+    t0 = time.perf_counter()
+    O.sweep_f32(STENCIL, [x], steps=1, lo=pad, hi=P - pad, coef=float(np.float32(1.0 / 7.0)))
+    one = time.perf_counter() - t0
+    k = max(1, min(100, int(target_s / max(one, 1e-3))))
+    t0 = time.perf_counter()
+    O.sweep_f32(STENCIL, [x], steps=k, lo=pad, hi=P - pad, coef=float(np.float32(1.0 / 7.0)))
+    el = time.perf_counter() - t0
+    return float(N) ** 3 * k / el / 1e9, k, el
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.set_threads(threads)
+    pad = 1
+    P = N + 2 * pad
+    x = O.fill_ref(3, P, pad, P - pad, 123456, 1)[0]
+    sample_steps = 2
+    coef = 1.0 / 7.0
+    for _ in range(args.warmup):
+        O.sweep_f32(STENCIL, [x], steps=1, lo=pad, hi=P - pad, coef=coef)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.sweep_f32(STENCIL, [x], steps=sample_steps, lo=pad, hi=P - pad, coef=coef)
+    el = time.perf_counter() - t0
+    v = float(N) ** 3 * sample_steps * args.steps / el / 1e9
+    sample = "512^3 x %d time steps per bench step (of the workload's 100), %d threads" % (
+        sample_steps, threads)
+    print(json.dumps({
+        "impl": "reference", "metric": "GUpdates/s", "value": v, "unit": "GUpdates/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (srand(123456) uniform [0,1))",
+        "config": {"workload": "jacobi-3d 7-point FP32, 512^3 interior, 100 steps, zero Dirichlet",
+                   "sample": sample},
+        "cpu_baseline": {"value": v, "unit": "GUpdates/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": v, "unit": "GUpdates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    world, rank, local = dist_setup()
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import ots
+
+    cfg, cfg_src = tuned_config()
+    plan = ots.Plan(STENCIL, N, STEPS, device=local, **cfg)
+    g = plan.geometry
+    state, aux = plan.fill_reference(seed=123456 + rank)
+    plan.upload(state, aux)
+    stream = torch.cuda.ExternalStream(plan.stream_ptr(), device=local)
+    launches_per_step = g.launches
+
+    def timed(kernel, k):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        barrier(world)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(k):
+            plan.run_async(kernel)
+        e1.record(stream)
+        plan.sync()
+        torch.cuda.synchronize()
+        barrier(world)
+        return e0.elapsed_time(e1) / 1e3
+
+    # warm-up
+    for _ in range(args.warmup):
+        plan.run_async(cfg["kernel"])
+    plan.sync()
+    with Clocks(local) as clk:
+        el = timed(cfg["kernel"], args.steps)
+    el_max = reduce_max(el, world)
+    updates = float(N) ** 3 * STEPS * args.steps * world
+    value = updates / el_max / 1e9
+    avg_launch = el / (args.steps * launches_per_step)
+
+    # plain one-step comparator (same plan, same data)
+    for _ in range(max(1, args.warmup // 3)):
+        plan.run_async("plain")
+    plan.sync()
+    el_plain = reduce_max(timed("plain", max(1, args.steps // 2)), world)
+    plain_value = float(N) ** 3 * STEPS * max(1, args.steps // 2) * world / el_plain / 1e9
+    # the z-streamed kernel at T=1 is the strongest one-step kernel we have
+    plain_best = plain_value
+    try:
+        p1 = ots.Plan(STENCIL, N, STEPS, device=local, kernel="stream", T=1, bx=cfg["bx"],
+                      by=cfg["by"], bz=1, E=cfg["E"])
+        p1.upload(state, aux)
+        s1 = torch.cuda.ExternalStream(p1.stream_ptr(), device=local)
+        for _ in range(2):
+            p1.run_async()
+        p1.sync()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s1)
+        for _ in range(max(1, args.steps // 2)):
+            p1.run_async()
+        e1.record(s1)
+        p1.sync()
+        t1 = reduce_max(e0.elapsed_time(e1) / 1e3, world)
+        stream_t1 = float(N) ** 3 * STEPS * max(1, args.steps // 2) * world / t1 / 1e9
+        plain_best = max(plain_best, stream_t1)
+        p1.close()
+    except Exception:
+        stream_t1 = None
+
+    # end to end through the C ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        host_in = [np.ascontiguousarray(s) for s in state]
+        host_out = [np.zeros_like(s) for s in state]
+        L = ots.lib()
+        for a in host_in + host_out:
+            ots.check(L.ots_host_register(a.ctypes.data, a.nbytes))
+        h2d = sum(a.nbytes for a in host_in)
+        d2h = sum(a.nbytes for a in host_out)
+        plan.upload(host_in, aux)
+        plan.run(cfg["kernel"])
+        plan.download(host_out)
+        barrier(world)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            plan.upload(host_in, aux)
+            plan.run(cfg["kernel"])
+            plan.download(host_out)
+        torch.cuda.synchronize()
+        t_e2e = reduce_max(time.perf_counter() - t0, world)
+        barrier(world)
+        for a in host_in + host_out:
+            L.ots_host_unregister(a.ctypes.data)
+        e2e = {"value": updates / t_e2e / 1e9, "unit": "GUpdates/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h}
+
+    peak, peak_src = peaks()
+    bytes_per_launch = BYTES_PER_UPDATE * float(N) ** 3
+    achieved = bytes_per_launch / avg_launch / 1e9
+    traffic = profile_traffic(cfg["kernel"])
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic,
+                "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs)",
+                "note": "achieved = compulsory 8 B/cell per launch; each launch advances T steps"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        try:
+            v, k, el_cpu = cpu_sample(1, 10.0)
+            cpu = {"value": v, "unit": "GUpdates/s", "cores": 1, "kind": "port",
+                   "sample": "512^3 x %d time steps (%.1f s), single thread" % (k, el_cpu)}
+        except Exception as e:  # report, never fake
+            cpu = {"value": None, "unit": "GUpdates/s", "cores": 1, "kind": "port",
+                   "sample": "failed: %s" % e}
+
+    line = {
+        "metric": "GUpdates/s", "value": value, "unit": "GUpdates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el_max / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: srand(123456) rand()/(RAND_MAX+1) interior, zero Dirichlet ring",
+        "config": {"workload": "jacobi-3d 7-point FP32, 512^3 interior, 100 steps, weight 1/7",
+                   "kernel": cfg["kernel"], "T": cfg["T"], "block": [cfg["bx"], cfg["by"], cfg["bz"]],
+                   "E": cfg["E"], "config_source": cfg_src, "parallelism": "replicas x%d" % world,
+                   "l2": "inputs larger than L2 (2 x 537 MB vs 126 MB); no flush"},
+        "plain": {"value": plain_value, "unit": "GUpdates/s", "kernel": "plain one-step",
+                  "stream_T1": stream_t1, "best_one_step": plain_best,
+                  "speedup_vs_best_one_step": value / plain_best if plain_best else None},
+        "gpu_launches": launches_per_step * args.steps,
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "clocks": clk.summary(),
+        "flops": {"per_update": FLOPS_PER_UPDATE,
+                  "tflops": value * FLOPS_PER_UPDATE / 1e3},
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    plan.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

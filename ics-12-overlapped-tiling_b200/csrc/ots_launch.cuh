@@ -1,0 +1,143 @@
+// ots_launch.cuh -- host launchers and per-stencil kernel tables.
+//
+// Every kernel is a template instantiation compiled ahead of time for
+// sm_100a (E, T and the stencil are template arguments); a plan picks its
+// instantiation from these tables, which is what replaces the reference's
+// per-run OpenCL source generation and JIT build
+// (opencl/jacobi-2d/jacobi-2d.cpp:162-173, 741-780).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <utility>
+
+#include "ots_stream.cuh"
+#include "ots_tile.cuh"
+
+namespace ots {
+
+constexpr int kMaxE = 16;       // tile kernel, 1D/2D
+constexpr int kMaxE3 = 8;       // tile kernel, 3D
+constexpr int kMaxT = 8;        // stream kernel levels
+constexpr int kStreamEs[3] = {1, 2, 4};
+
+using TileLaunch = cudaError_t (*)(const StepParams&, dim3, dim3, size_t, cudaStream_t);
+using StreamLaunch = cudaError_t (*)(const CUtensorMap&, const StreamParams&, dim3, dim3, size_t,
+                                     cudaStream_t);
+using AttrFn = cudaError_t (*)(cudaFuncAttributes*);
+using OccFn = cudaError_t (*)(int*, int, size_t);
+
+struct StencilKernels {
+  TileLaunch tile[3][kMaxE + 1] = {};  // [E axis][E]
+  AttrFn tile_attr[3][kMaxE + 1] = {};
+  TileLaunch plain = nullptr;
+  AttrFn plain_attr = nullptr;
+  StreamLaunch stream[kMaxT + 1][3] = {};  // [T][index of E in kStreamEs]
+  AttrFn stream_attr[kMaxT + 1][3] = {};
+  OccFn stream_occ[kMaxT + 1][3] = {};
+  bool has_stream = false;
+};
+
+template <class K>
+inline cudaError_t ensure_smem(K kernel, size_t smem, std::atomic<size_t>& cached) {
+  if (smem <= 48 * 1024 || smem <= cached.load(std::memory_order_relaxed)) return cudaSuccess;
+  cudaError_t e =
+      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) cached.store(smem, std::memory_order_relaxed);
+  return e;
+}
+
+template <class Op, int E, int EAX>
+cudaError_t launch_tile(const StepParams& p, dim3 g, dim3 b, size_t smem, cudaStream_t s) {
+  static std::atomic<size_t> cached{0};
+  cudaError_t e = ensure_smem(tile_kernel<Op, E, EAX>, smem, cached);
+  if (e != cudaSuccess) return e;
+  tile_kernel<Op, E, EAX><<<g, b, smem, s>>>(p);
+  return cudaGetLastError();
+}
+
+template <class Op, int E, int EAX>
+cudaError_t attr_tile(cudaFuncAttributes* a) {
+  return cudaFuncGetAttributes(a, tile_kernel<Op, E, EAX>);
+}
+
+template <class Op>
+cudaError_t launch_plain(const StepParams& p, dim3 g, dim3 b, size_t, cudaStream_t s) {
+  plain_kernel<Op><<<g, b, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+template <class Op>
+cudaError_t attr_plain(cudaFuncAttributes* a) {
+  return cudaFuncGetAttributes(a, plain_kernel<Op>);
+}
+
+template <class Op, int T, int E>
+cudaError_t launch_stream(const CUtensorMap& m, const StreamParams& p, dim3 g, dim3 b,
+                          size_t smem, cudaStream_t s) {
+  static std::atomic<size_t> cached{0};
+  cudaError_t e = ensure_smem(stream_kernel<Op, T, E>, smem, cached);
+  if (e != cudaSuccess) return e;
+  stream_kernel<Op, T, E><<<g, b, smem, s>>>(m, p);
+  return cudaGetLastError();
+}
+
+template <class Op, int T, int E>
+cudaError_t attr_stream(cudaFuncAttributes* a) {
+  return cudaFuncGetAttributes(a, stream_kernel<Op, T, E>);
+}
+
+template <class Op, int T, int E>
+cudaError_t occ_stream(int* blocks, int threads, size_t smem) {
+  static std::atomic<size_t> cached{0};
+  cudaError_t e = ensure_smem(stream_kernel<Op, T, E>, smem, cached);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, stream_kernel<Op, T, E>, threads,
+                                                       smem);
+}
+
+template <class Op, int EAX, int... Es>
+void fill_tile(StencilKernels& k, std::integer_sequence<int, Es...>) {
+  ((k.tile[EAX][Es + 1] = &launch_tile<Op, Es + 1, EAX>,
+    k.tile_attr[EAX][Es + 1] = &attr_tile<Op, Es + 1, EAX>),
+   ...);
+}
+
+template <class Op, int EI, int... Ts>
+void fill_stream_e(StencilKernels& k, std::integer_sequence<int, Ts...>) {
+  ((k.stream[Ts + 1][EI] = &launch_stream<Op, Ts + 1, kStreamEs[EI]>,
+    k.stream_attr[Ts + 1][EI] = &attr_stream<Op, Ts + 1, kStreamEs[EI]>,
+    k.stream_occ[Ts + 1][EI] = &occ_stream<Op, Ts + 1, kStreamEs[EI]>),
+   ...);
+}
+
+template <class Op>
+StencilKernels make_kernels() {
+  StencilKernels k;
+  if constexpr (Op::DIMS == 1) fill_tile<Op, 0>(k, std::make_integer_sequence<int, kMaxE>{});
+  if constexpr (Op::DIMS == 2) fill_tile<Op, 1>(k, std::make_integer_sequence<int, kMaxE>{});
+  if constexpr (Op::DIMS == 3) {
+    fill_tile<Op, 2>(k, std::make_integer_sequence<int, kMaxE3>{});
+    fill_tile<Op, 1>(k, std::make_integer_sequence<int, kMaxE3>{});
+  }
+  k.plain = &launch_plain<Op>;
+  k.plain_attr = &attr_plain<Op>;
+  return k;
+}
+
+template <class Op>
+StencilKernels make_kernels_with_stream() {
+  StencilKernels k = make_kernels<Op>();
+  fill_stream_e<Op, 0>(k, std::make_integer_sequence<int, kMaxT>{});
+  fill_stream_e<Op, 1>(k, std::make_integer_sequence<int, kMaxT>{});
+  fill_stream_e<Op, 2>(k, std::make_integer_sequence<int, kMaxT>{});
+  k.has_stream = true;
+  return k;
+}
+
+// Defined one per stencil in ots_k_<stencil>.cu.
+const StencilKernels& kernels_for(int stencil);
+
+}  // namespace ots

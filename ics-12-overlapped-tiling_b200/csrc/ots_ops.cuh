@@ -1,0 +1,318 @@
+// ots_ops.cuh -- per-point updates of the thirteen stencils.
+//
+// Every stencil is written as ONE fused update of its evolving fields from
+// the previous time level, so that every kernel family (overlapped tile,
+// z-streamed tile, plain one-step) shares the same arithmetic.  Multi-phase
+// reference kernels are fused by recomputing the first phase at the
+// neighbours the second phase reads: fdtd-2d recomputes E' at x+1 and y+1
+// (opencl/fdtd-2d/fdtd-2d.cpp:267-330), rician-denoise-2d recomputes g at the
+// four neighbours (opencl/rician-denoise-2d/rician-denoise-2d.cpp:271-329).
+// Recomputation repeats the identical operations, so the fused result is bit
+// for bit the phased one.
+//
+// Operand order follows the reference exactly (the CPU loops where they are
+// correct, else the generated kernels).  The library is compiled with
+// -fmad=false, so every + and * is its own IEEE single operation and linear
+// stencils reproduce the CPU result exactly.  1/sqrt terms use rsqrtf as the
+// reference kernels used OpenCL rsqrt.
+//
+// Accessor contract (A):   a(f, dz, dy, dx)      state field f at an offset
+//                          a.inside(dz, dy, dx)  is that cell in the domain
+// Cells outside the domain hold 0 for every field (zero Dirichlet ring).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#if defined(__CUDACC__)
+#define OTS_HD __host__ __device__ __forceinline__
+#else
+#define OTS_HD inline
+#endif
+
+namespace ots {
+
+// 1/sqrt: the rsqrt intrinsic on the GPU (as the reference kernels used
+// OpenCL rsqrt); on the host (the runner's own -v check) 1/sqrtf.
+OTS_HD float ots_rsqrt(float v) {
+#if defined(__CUDA_ARCH__)
+  return rsqrtf(v);
+#else
+  return 1.0f / sqrtf(v);
+#endif
+}
+
+struct OpArgs {
+  float coef;   // averaging weight
+  float h2;     // Poisson h^2
+  int variant;  // 0 baseline, 1 reference arithmetic
+};
+
+OTS_HD float sq(float v) { return v * v; }
+
+// ---------------------------------------------------------------- 1D ----
+
+// opencl/jacobi-1d/jacobi-1d.cpp:635-637
+struct OpJacobi1D {
+  static constexpr int DIMS = 1, NS = 1, NA = 0, RX = 1, RY = 0, RZ = 0;
+  static constexpr bool STAR = false;
+  template <class A>
+  OTS_HD static void apply(const A& a, const float*, const OpArgs& p, int,
+                                               float* o) {
+    o[0] = p.coef * (a(0, 0, 0, -1) + a(0, 0, 0, 0) + a(0, 0, 0, 1));
+  }
+};
+
+// opencl/jacobi-1d-5pt/jacobi-1d-5pt.cpp:507-511 (CPU arithmetic; the
+// generated kernel's step 1 is defective, jacobi-1d-5pt.cpp:197-206)
+struct OpJacobi1D5 {
+  static constexpr int DIMS = 1, NS = 1, NA = 0, RX = 2, RY = 0, RZ = 0;
+  static constexpr bool STAR = false;
+  template <class A>
+  OTS_HD static void apply(const A& a, const float*, const OpArgs& p, int,
+                                               float* o) {
+    o[0] = p.coef *
+           (a(0, 0, 0, -2) + a(0, 0, 0, -1) + a(0, 0, 0, 0) + a(0, 0, 0, 1) + a(0, 0, 0, 2));
+  }
+};
+
+// opencl/jacobi-1d-7pt/jacobi-1d-7pt.cpp:515-521 (weight 0.2f as written)
+struct OpJacobi1D7 {
+  static constexpr int DIMS = 1, NS = 1, NA = 0, RX = 3, RY = 0, RZ = 0;
+  static constexpr bool STAR = false;
+  template <class A>
+  OTS_HD static void apply(const A& a, const float*, const OpArgs& p, int,
+                                               float* o) {
+    o[0] = p.coef * (a(0, 0, 0, -3) + a(0, 0, 0, -2) + a(0, 0, 0, -1) + a(0, 0, 0, 0) +
+                     a(0, 0, 0, 1) + a(0, 0, 0, 2) + a(0, 0, 0, 3));
+  }
+};
+
+// ---------------------------------------------------------------- 2D ----
+
+// opencl/jacobi-2d/jacobi-2d.cpp:824-828: (1/5)(l + c + r + t + b)
+struct OpJacobi2D {
+  static constexpr int DIMS = 2, NS = 1, NA = 0, RX = 1, RY = 1, RZ = 0;
+  static constexpr bool STAR = true;
+  template <class A>
+  OTS_HD static void apply(const A& a, const float*, const OpArgs& p, int,
+                                               float* o) {
+    o[0] = p.coef *
+           (a(0, 0, 0, -1) + a(0, 0, 0, 0) + a(0, 0, 0, 1) + a(0, 0, -1, 0) + a(0, 0, 1, 0));
+  }
+};
+
+// Reference: opencl/poisson-2d/poisson-2d.cpp:644-648, 8c - (8 neighbours).
+// Baseline: Jacobi sweep for the 5-point Poisson problem, (sum4 - h^2 f)/4.
+struct OpPoisson2D {
+  static constexpr int DIMS = 2, NS = 1, NA = 1, RX = 1, RY = 1, RZ = 0;
+  static constexpr bool STAR = false;
+  template <class A>
+  OTS_HD static void apply(const A& a, const float* aux, const OpArgs& p,
+                                               int, float* o) {
+    if (p.variant == 1) {
+      o[0] = 8.0f * a(0, 0, 0, 0) -
+             (a(0, 0, -1, -1) + a(0, 0, -1, 0) + a(0, 0, -1, 1) + a(0, 0, 0, -1) +
+              a(0, 0, 0, 1) + a(0, 0, 1, -1) + a(0, 0, 1, 0) + a(0, 0, 1, 1));
+    } else {
+      float s = a(0, 0, -1, 0) + a(0, 0, 0, -1) + a(0, 0, 0, 1) + a(0, 0, 1, 0);
+      o[0] = (s - p.h2 * aux[0]) * 0.25f;
+    }
+  }
+};
+
+// opencl/gradient-2d/gradient-2d.cpp:283-289: c + rsqrt(1e-4 + sum (c-n)^2)
+struct OpGradient2D {
+  static constexpr int DIMS = 2, NS = 1, NA = 0, RX = 1, RY = 1, RZ = 0;
+  static constexpr bool STAR = true;
+  template <class A>
+  OTS_HD static void apply(const A& a, const float*, const OpArgs&, int,
+                                               float* o) {
+    float c = a(0, 0, 0, 0);
+    o[0] = c + ots_rsqrt(0.0001f + sq(c - a(0, 0, 0, -1)) + sq(c - a(0, 0, 0, 1)) +
+                      sq(c - a(0, 0, -1, 0)) + sq(c - a(0, 0, 1, 0)));
+  }
+};
+
+// Fields: 0 Ex, 1 Ey, 2 Hz.  opencl/fdtd-2d/fdtd-2d.cpp:267-330.
+// Baseline: standard sign (Hz -= 0.7(dEx/dx + dEy/dy)) and Ey on interior row
+// 0 driven to the global step index.  Reference: "+Ey" (fdtd-2d.cpp:322), no
+// source.
+struct OpFdtd2D {
+  static constexpr int DIMS = 2, NS = 3, NA = 0, RX = 1, RY = 1, RZ = 0;
+  static constexpr bool STAR = false;
+  template <class A>
+  OTS_HD static float ey_new(const A& a, const OpArgs& p, int t, int dy,
+                                                 int dx) {
+    if (!a.inside(0, dy, dx)) return 0.0f;
+    if (p.variant == 0 && a.gy() + dy == 0) return (float)t;
+    return a(1, 0, dy, dx) - 0.5f * (a(2, 0, dy, dx) - a(2, 0, dy - 1, dx));
+  }
+  template <class A>
+  OTS_HD static float ex_new(const A& a, int dy, int dx) {
+    if (!a.inside(0, dy, dx)) return 0.0f;
+    return a(0, 0, dy, dx) - 0.5f * (a(2, 0, dy, dx) - a(2, 0, dy, dx - 1));
+  }
+  template <class A>
+  OTS_HD static void apply(const A& a, const float*, const OpArgs& p, int t,
+                                               float* o) {
+    float ey = ey_new(a, p, t, 0, 0);
+    float ex = ex_new(a, 0, 0);
+    float exr = ex_new(a, 0, 1);
+    float eyb = ey_new(a, p, t, 1, 0);
+    float d = (exr - ex) + eyb;
+    d = (p.variant == 1) ? d + ey : d - ey;
+    o[0] = ex;
+    o[1] = ey;
+    o[2] = a(2, 0, 0, 0) - 0.7f * d;
+  }
+};
+
+// opencl/rician-denoise-2d/rician-denoise-2d.cpp:153-161 constants, :271-329
+// arithmetic; aux 0 = F (the noisy image).
+struct OpRician2D {
+  static constexpr int DIMS = 2, NS = 1, NA = 1, RX = 2, RY = 2, RZ = 0;
+  static constexpr bool STAR = false;
+  template <class A>
+  OTS_HD static float g_at(const A& a, int dy, int dx) {
+    if (!a.inside(0, dy, dx)) return 0.0f;
+    float c = a(0, 0, dy, dx);
+    return ots_rsqrt(1.0E-20f + sq(c - a(0, 0, dy, dx + 1)) + sq(c - a(0, 0, dy, dx - 1)) +
+                  sq(c - a(0, 0, dy + 1, dx)) + sq(c - a(0, 0, dy - 1, dx)));
+  }
+  template <class A>
+  OTS_HD static void apply(const A& a, const float* aux, const OpArgs&, int,
+                                               float* o) {
+    const float DT = 5.0f, SIGMA2 = 0.0025f, GAMMA = 0.065f / 0.0025f;
+    float c = a(0, 0, 0, 0), f = aux[0];
+    float r = c * f / SIGMA2;
+    r = (r * (2.38944f + r * (0.950037f + r))) / (4.65314f + r * (2.57541f + r * (1.48937f + r)));
+    float gl = g_at(a, 0, -1), gr = g_at(a, 0, 1), gt = g_at(a, -1, 0), gb = g_at(a, 1, 0);
+    float ugl = a(0, 0, 0, -1) * gl, ugr = a(0, 0, 0, 1) * gr, ugt = a(0, 0, -1, 0) * gt,
+          ugb = a(0, 0, 1, 0) * gb;
+    o[0] = (c + DT * (ugb + ugt + ugr + ugl + GAMMA * f * r)) /
+           (1.0f + DT * (gr + gl + gb + gt + GAMMA));
+  }
+};
+
+// opencl/cdsc-tv-update-2d/cdsc-tv-update-2d.cpp:163-164, :287-309;
+// aux 0 = F, aux 1 = V.
+struct OpTvUpdate2D {
+  static constexpr int DIMS = 2, NS = 1, NA = 2, RX = 1, RY = 1, RZ = 0;
+  static constexpr bool STAR = false;
+  template <class A>
+  OTS_HD static void apply(const A& a, const float* aux, const OpArgs&, int,
+                                               float* o) {
+    const float EPI1 = 1e-8f, ALPHA = 1.1f;
+    float tc = a(0, 0, -1, 0), tr = a(0, 0, -1, 1), ml = a(0, 0, 0, -1), mc = a(0, 0, 0, 0),
+          mr = a(0, 0, 0, 1), bl = a(0, 0, 1, -1), bc = a(0, 0, 1, 0);
+    float F = aux[0], V = aux[1];
+    float c1 = mc * ots_rsqrt(EPI1 + ((bc - mc) * (bc - mc)) + ((mr - mc) * (mr - mc))) / V;
+    float c2 = mc * ots_rsqrt(EPI1 + ((mc - tc) * (mc - tc)) + ((tr - tc) * (tr - tc))) / V;
+    float c3 = mc * ots_rsqrt(EPI1 + ((bc - mc) * (bc - mc)) + ((mr - mc) * (mr - mc))) / V;
+    float c4 = mc * ots_rsqrt(EPI1 + ((bl - ml) * (bl - ml)) + ((mc - ml) * (mc - ml))) / V;
+    o[0] = 1.0f / (ALPHA + c1 + c2 + c3 + c4) * (ALPHA * F + c1 * bc + c2 * tc + c3 * mr + c4 * ml);
+  }
+};
+
+// ---------------------------------------------------------------- 3D ----
+
+// Generated-kernel operand order (opencl/jacobi-3d/jacobi-3d.cpp:282-304):
+// x-1, c, x+1, y-1, y+1, z-1, z+1.
+struct OpJacobi3D {
+  static constexpr int DIMS = 3, NS = 1, NA = 0, RX = 1, RY = 1, RZ = 1;
+  static constexpr bool STAR = true;
+  template <class A>
+  OTS_HD static void apply(const A& a, const float*, const OpArgs& p, int,
+                                               float* o) {
+    o[0] = p.coef * (a(0, 0, 0, -1) + a(0, 0, 0, 0) + a(0, 0, 0, 1) + a(0, 0, -1, 0) +
+                     a(0, 0, 1, 0) + a(0, -1, 0, 0) + a(0, 1, 0, 0));
+  }
+  // Same arithmetic from the seven values (used by the z-streamed kernels).
+  OTS_HD static float star(float xm, float c, float xp, float ym, float yp,
+                                               float zm, float zp, float, const OpArgs& p) {
+    return p.coef * (xm + c + xp + ym + yp + zm + zp);
+  }
+};
+
+// Reference: opencl/poisson-3d/poisson-3d.cpp:280-293, 26c - (26 neighbours,
+// x outer, y, z inner).  Baseline: Jacobi sweep for the 7-point Poisson
+// problem with RHS f: (x-1 + x+1 + y-1 + y+1 + z-1 + z+1 - h^2 f) * (1/6).
+struct OpPoisson3D {
+  static constexpr int DIMS = 3, NS = 1, NA = 1, RX = 1, RY = 1, RZ = 1;
+  static constexpr bool STAR = true;  // star only in the baseline variant
+  template <class A>
+  OTS_HD static void apply(const A& a, const float* aux, const OpArgs& p,
+                                               int, float* o) {
+    if (p.variant == 1) {
+      float s = 0.0f;
+      bool first = true;
+#pragma unroll
+      for (int ox = -1; ox <= 1; ++ox)
+#pragma unroll
+        for (int oy = -1; oy <= 1; ++oy)
+#pragma unroll
+          for (int oz = -1; oz <= 1; ++oz) {
+            if (ox == 0 && oy == 0 && oz == 0) continue;
+            float v = a(0, oz, oy, ox);
+            s = first ? v : s + v;
+            first = false;
+          }
+      o[0] = 26.0f * a(0, 0, 0, 0) - s;
+    } else {
+      float s = a(0, 0, 0, -1) + a(0, 0, 0, 1) + a(0, 0, -1, 0) + a(0, 0, 1, 0) +
+                a(0, -1, 0, 0) + a(0, 1, 0, 0);
+      o[0] = (s - p.h2 * aux[0]) * (1.0f / 6.0f);
+    }
+  }
+  OTS_HD static float star(float xm, float, float xp, float ym, float yp,
+                                               float zm, float zp, float f, const OpArgs& p) {
+    float s = xm + xp + ym + yp + zm + zp;
+    return (s - p.h2 * f) * (1.0f / 6.0f);
+  }
+};
+
+// opencl/gradient-3d/gradient-3d.cpp:305-307
+struct OpGradient3D {
+  static constexpr int DIMS = 3, NS = 1, NA = 0, RX = 1, RY = 1, RZ = 1;
+  static constexpr bool STAR = true;
+  template <class A>
+  OTS_HD static void apply(const A& a, const float*, const OpArgs&, int,
+                                               float* o) {
+    float c = a(0, 0, 0, 0);
+    o[0] = c + ots_rsqrt(0.0001f + sq(c - a(0, 0, 0, -1)) + sq(c - a(0, 0, 0, 1)) +
+                      sq(c - a(0, 0, -1, 0)) + sq(c - a(0, 0, 1, 0)) + sq(c - a(0, -1, 0, 0)) +
+                      sq(c - a(0, 1, 0, 0)));
+  }
+  OTS_HD static float star(float xm, float c, float xp, float ym, float yp,
+                                               float zm, float zp, float, const OpArgs&) {
+    return c + ots_rsqrt(0.0001f + sq(c - xm) + sq(c - xp) + sq(c - ym) + sq(c - yp) +
+                      sq(c - zm) + sq(c - zp));
+  }
+};
+
+// opencl/cs-3d/cs-3d.cpp:161-163 constants, :284-308 arithmetic with y+1 as
+// the "p1" direction throughout (the reference's step-1 code flips it).
+struct OpCs3D {
+  static constexpr int DIMS = 3, NS = 1, NA = 0, RX = 1, RY = 1, RZ = 1;
+  static constexpr bool STAR = false;
+  template <class A>
+  OTS_HD static void apply(const A& a, const float*, const OpArgs&, int,
+                                               float* o) {
+    const float EPS = 1e-9f, SUMAREF = 1.1f, ALPHA = 1.1f;
+    float u = a(0, 0, 0, 0);
+    float zp = a(0, 1, 0, 0), zm = a(0, -1, 0, 0), yp = a(0, 0, 1, 0), ym = a(0, 0, -1, 0),
+          xp = a(0, 0, 0, 1), xm = a(0, 0, 0, -1);
+    float zm_yp = a(0, -1, 1, 0), zm_xp = a(0, -1, 0, 1), zp_ym = a(0, 1, -1, 0),
+          ym_xp = a(0, 0, -1, 1), zp_xm = a(0, 1, 0, -1), yp_xm = a(0, 0, 1, -1);
+    float c1 = u * ots_rsqrt(EPS + sq(zp - u) + sq(yp - u) + sq(xp - u)) / SUMAREF;
+    float c2 = u * ots_rsqrt(EPS + sq(u - zm) + sq(zm_yp - zm) + sq(zm_xp - zm)) / SUMAREF;
+    float c3 = u * ots_rsqrt(EPS + sq(zp_ym - ym) + sq(u - ym) + sq(ym_xp - ym)) / SUMAREF;
+    float c4 = u * ots_rsqrt(EPS + sq(zp_xm - xm) + sq(yp_xm - xm) + sq(u - xm)) / SUMAREF;
+    o[0] = (ALPHA * u + c1 * (zp + yp + xp) + c2 * zm + c3 * ym + c4 * xm) /
+           (ALPHA + 3.0f * c1 + c2 + c3 + c4);
+  }
+};
+
+}  // namespace ots

@@ -1,0 +1,226 @@
+// ots_tile.cuh -- overlapped time-tile kernel (all dimensions) and the plain
+// one-step-per-launch kernel.
+//
+// The overlapped tile follows the reference scheme
+// (opencl/jacobi-2d/jacobi-2d.cpp:197-514): a CTA of (bx, by, bz) threads,
+// each owning E cells along one axis, computes a tile of comps cells, of which
+// the inner real_per_block = comps - 2r(T-1) cells per axis are exact after T
+// steps and are the only ones written back.  Differences from the reference,
+// B200-first:
+//   * the whole halo-extended tile (comps + 2r per axis) is loaded once into
+//     shared memory with coalesced loads, and T steps run there ping-ponging
+//     two shared buffers, one barrier per step (the reference does step 1 from
+//     global memory and then two barriers per step);
+//   * cells outside the domain read as zero through predicated loads, so the
+//     device arrays hold only the interior (no ring), and the problem size
+//     need not be a multiple of real_per_block (partial edge tiles);
+//   * the write-back respects all axes, including z (the reference ignores
+//     writeValidZ, opencl/jacobi-3d/jacobi-3d.cpp:400-405).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "ots_ops.cuh"
+
+namespace ots {
+
+// Device layout of one field: x fastest, rows of `sy` floats (sy >= n0,
+// 128-byte aligned), planes of `sz` floats.
+struct Layout {
+  int n0, n1, n2;  // interior extent per axis (1 for unused axes)
+  int64_t sy, sz;
+};
+
+struct StepParams {
+  const float* in[3];
+  float* out[3];
+  const float* aux[2];
+  Layout L;
+  int rpb[3];        // interior cells written per CTA and axis
+  int T;             // time steps per launch
+  int steps;         // total steps of the run
+  int base_step;     // global index of this launch's first step
+  int phase_limit;   // 0 full, 1/2/3 partial kernels (reference -p)
+  OpArgs op;
+};
+
+__device__ __forceinline__ bool in_domain(const Layout& L, int x, int y, int z) {
+  return (unsigned)x < (unsigned)L.n0 && (unsigned)y < (unsigned)L.n1 &&
+         (unsigned)z < (unsigned)L.n2;
+}
+
+// Accessor over a shared-memory tile (fields `fs` floats apart).
+struct SmemAcc {
+  const float* p;
+  int fs, sy, sz;
+  int x, y, z;
+  Layout L;
+  __device__ __forceinline__ float operator()(int f, int dz, int dy, int dx) const {
+    return p[f * fs + dz * sz + dy * sy + dx];
+  }
+  __device__ __forceinline__ bool inside(int dz, int dy, int dx) const {
+    return in_domain(L, x + dx, y + dy, z + dz);
+  }
+  __device__ __forceinline__ int gy() const { return y; }
+};
+
+// Accessor over global memory with zero outside the domain.
+template <int NS>
+struct GmemAcc {
+  const float* f[NS];
+  int64_t i;
+  int x, y, z;
+  Layout L;
+  __device__ __forceinline__ float operator()(int fi, int dz, int dy, int dx) const {
+    return inside(dz, dy, dx) ? __ldg(f[fi] + i + dz * L.sz + dy * L.sy + dx) : 0.0f;
+  }
+  __device__ __forceinline__ bool inside(int dz, int dy, int dx) const {
+    return in_domain(L, x + dx, y + dy, z + dz);
+  }
+  __device__ __forceinline__ int gy() const { return y; }
+};
+
+// ------------------------------------------------------------------------
+// Overlapped tile: E cells per thread along axis EAX.  E is contiguous per
+// thread along y/z (register reuse of the shared neighbours) and strided by
+// the block size along x (the reference 1D scheme, jacobi-1d.cpp:249-256,
+// which keeps warps on consecutive addresses).
+// ------------------------------------------------------------------------
+// Threads per CTA shrink as E grows so that the E-cell register blocks do
+// not spill; the host rejects larger blocks with OTS_ERR_BLOCK_TOO_LARGE.
+template <int E, int NS>
+struct TileThreads {
+  static constexpr int kMax = (E * NS <= 2) ? 1024 : (E * NS <= 4) ? 512 : 256;
+};
+
+template <class Op, int E, int EAX>
+__global__ void __launch_bounds__(TileThreads<E, Op::NS>::kMax) tile_kernel(const StepParams p) {
+  constexpr int NS = Op::NS, NA = Op::NA;
+  constexpr int RX = Op::RX, RY = Op::RY, RZ = Op::RZ;
+  extern __shared__ float smem[];
+  const int bx = blockDim.x, by = blockDim.y, bz = blockDim.z;
+  const int cx = bx * (EAX == 0 ? E : 1);
+  const int cy = by * (EAX == 1 ? E : 1);
+  const int cz = bz * (EAX == 2 ? E : 1);
+  const int Lx = cx + 2 * RX, Ly = cy + 2 * RY, Lz = cz + 2 * RZ;
+  const int LxLy = Lx * Ly, Lvol = LxLy * Lz;
+  const int T = p.T;
+  // global coordinate of comps cell 0
+  const int ox = blockIdx.x * p.rpb[0] - RX * (T - 1);
+  const int oy = blockIdx.y * p.rpb[1] - RY * (T - 1);
+  const int oz = blockIdx.z * p.rpb[2] - RZ * (T - 1);
+  const int tid = threadIdx.x + bx * (threadIdx.y + by * threadIdx.z);
+  const int nth = bx * by * bz;
+  if (p.phase_limit == 1) return;
+
+  float* cur = smem;
+  float* nxt = smem + NS * Lvol;
+  if (p.phase_limit != 3) {
+    for (int i = tid; i < Lvol; i += nth) {
+      const int lz = i / LxLy;
+      const int rem = i - lz * LxLy;
+      const int ly = rem / Lx;
+      const int lx = rem - ly * Lx;
+      const int gx = ox - RX + lx, gy = oy - RY + ly, gz = oz - RZ + lz;
+      const bool in = in_domain(p.L, gx, gy, gz);
+      const int64_t gi = (int64_t)gz * p.L.sz + (int64_t)gy * p.L.sy + gx;
+#pragma unroll
+      for (int f = 0; f < NS; ++f) {
+        const float v = in ? __ldg(p.in[f] + gi) : 0.0f;
+        cur[f * Lvol + i] = v;
+        nxt[f * Lvol + i] = v;  // the ring of the second buffer stays defined
+      }
+    }
+  }
+
+  // Owned cells.
+  int sidx[E], gxs[E], gys[E], gzs[E];
+  bool ins[E];
+  float auxv[E][NA > 0 ? NA : 1];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    int lx = threadIdx.x, ly = threadIdx.y, lz = threadIdx.z;
+    if (EAX == 0) lx = threadIdx.x + e * bx;
+    if (EAX == 1) ly = threadIdx.y * E + e;
+    if (EAX == 2) lz = threadIdx.z * E + e;
+    sidx[e] = (lz + RZ) * LxLy + (ly + RY) * Lx + (lx + RX);
+    gxs[e] = ox + lx;
+    gys[e] = oy + ly;
+    gzs[e] = oz + lz;
+    ins[e] = in_domain(p.L, gxs[e], gys[e], gzs[e]);
+    const int64_t gi = (int64_t)gzs[e] * p.L.sz + (int64_t)gys[e] * p.L.sy + gxs[e];
+#pragma unroll
+    for (int a = 0; a < NA; ++a) auxv[e][a] = ins[e] ? __ldg(p.aux[a] + gi) : 0.0f;
+  }
+  __syncthreads();
+
+  int nsteps = p.steps - p.base_step;
+  if (nsteps > T) nsteps = T;
+  for (int s = 0; s < nsteps; ++s) {
+    float res[E][NS];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      SmemAcc acc{cur + sidx[e], Lvol, Lx, LxLy, gxs[e], gys[e], gzs[e], p.L};
+      Op::apply(acc, auxv[e], p.op, p.base_step + s, res[e]);
+#pragma unroll
+      for (int f = 0; f < NS; ++f)
+        if (!ins[e]) res[e][f] = 0.0f;
+    }
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+#pragma unroll
+      for (int f = 0; f < NS; ++f) nxt[f * Lvol + sidx[e]] = res[e][f];
+    __syncthreads();
+    float* t = cur;
+    cur = nxt;
+    nxt = t;
+    if (p.phase_limit == 2) return;
+  }
+  if (p.phase_limit == 3) return;
+
+  // Interior write-back: comps coordinate in [r(T-1), r(T-1) + rpb) per axis.
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int lx = gxs[e] - ox, ly = gys[e] - oy, lz = gzs[e] - oz;
+    const bool w = lx >= RX * (T - 1) && lx < RX * (T - 1) + p.rpb[0] && ly >= RY * (T - 1) &&
+                   ly < RY * (T - 1) + p.rpb[1] && lz >= RZ * (T - 1) &&
+                   lz < RZ * (T - 1) + p.rpb[2];
+    if (w && ins[e]) {
+      const int64_t gi = (int64_t)gzs[e] * p.L.sz + (int64_t)gys[e] * p.L.sy + gxs[e];
+#pragma unroll
+      for (int f = 0; f < NS; ++f) p.out[f][gi] = cur[f * Lvol + sidx[e]];
+    }
+  }
+}
+
+// ------------------------------------------------------------------------
+// Plain kernel: one time step per launch, one cell per thread, neighbours
+// straight from global memory (L1/L2).  Grid covers the interior exactly.
+// ------------------------------------------------------------------------
+template <class Op>
+__global__ void __launch_bounds__(256) plain_kernel(const StepParams p) {
+  constexpr int NS = Op::NS, NA = Op::NA;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z * blockDim.z + threadIdx.z;
+  if (!in_domain(p.L, x, y, z)) return;
+  const int64_t i = (int64_t)z * p.L.sz + (int64_t)y * p.L.sy + x;
+  float auxv[NA > 0 ? NA : 1];
+#pragma unroll
+  for (int a = 0; a < NA; ++a) auxv[a] = __ldg(p.aux[a] + i);
+  GmemAcc<NS> acc;
+#pragma unroll
+  for (int f = 0; f < NS; ++f) acc.f[f] = p.in[f];
+  acc.i = i;
+  acc.x = x;
+  acc.y = y;
+  acc.z = z;
+  acc.L = p.L;
+  float res[NS];
+  Op::apply(acc, auxv, p.op, p.base_step, res);
+#pragma unroll
+  for (int f = 0; f < NS; ++f) p.out[f][i] = res[f];
+}
+
+}  // namespace ots

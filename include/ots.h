@@ -1,0 +1,241 @@
+/*
+ * ots.h -- C ABI of the overlapped time-tiling stencil engine (libots.so).
+ *
+ * One B200, FP32, thirteen stencils.  The entry points take the parameter
+ * surface of the reference's kernel-generator-plus-runner programs
+ * (jholewinski/ics-12-overlapped-tiling, opencl/<stencil>/<stencil>.cpp) and
+ * replace, in one library, what each runner did by hand:
+ *
+ *   reference                                         here
+ *   ---------------------------------------------    ------------------------
+ *   GeneratorParams + computeDerived()                ots_plan_create,
+ *     (opencl/jacobi-2d/jacobi-2d.cpp:21-127)           ots_plan_geometry
+ *   XGenerator::generate() -> OpenCL source,          compiled sm_100a kernels
+ *     cl::Program::build                                chosen by ots_plan_create
+ *     (opencl/jacobi-2d/jacobi-2d.cpp:162-173,741-780)
+ *   hostData fill + enqueueWriteBuffer x2             ots_fill_reference,
+ *     (opencl/jacobi-2d/jacobi-2d.cpp:787-802,874-886)  ots_upload
+ *   launch loop, swap(in,out), events, rtclock        ots_run
+ *     (opencl/jacobi-2d/jacobi-2d.cpp:899-948)
+ *   enqueueReadBuffer(*inputBuffer)                   ots_download
+ *     (opencl/jacobi-2d/jacobi-2d.cpp:952-954)
+ *   printProgramParameters + printValue keys          ots_describe
+ *     (opencl/common/inc/ProgramGenerator.hpp:19-66)
+ *   CLContext (opencl/common/src/CLContext.cpp:11-45) ots_device_info
+ *   throwOnError (CLContext.cpp:50-56), "ERROR: ..."  ots_status +
+ *     (opencl/jacobi-2d/jacobi-2d.cpp:682-690)          ots_last_error
+ *
+ * Host arrays use the reference layout: P^d floats per field, x fastest,
+ * P = ots_geometry.padded_size, interior cells at [padding, padding+real_size)
+ * on every axis, every other cell zero (zero Dirichlet ring).  Device arrays
+ * are plan-owned.  No call throws; every call returns an ots_status and
+ * records a message for ots_last_error() (per thread).
+ *
+ * Threading: a plan is used by one host thread at a time; distinct plans may
+ * be used concurrently from distinct threads.
+ */
+#ifndef OTS_H
+#define OTS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum ots_status {
+  OTS_OK = 0,
+  OTS_ERR_INVALID_ARGUMENT = 1,
+  OTS_ERR_INVALID_GEOMETRY = 2, /* reference: "Consistency error!" / assert */
+  OTS_ERR_SMEM_TOO_LARGE = 3,   /* reference: "Not enough local memory ..." */
+  OTS_ERR_BLOCK_TOO_LARGE = 4,  /* reference: "Block dimensions are too large!" */
+  OTS_ERR_CUDA = 5,
+  OTS_ERR_TIMEOUT = 6,          /* a bounded device wait gave up */
+  OTS_ERR_UNSUPPORTED = 7,
+  OTS_ERR_NO_DEVICE = 8,
+  OTS_ERR_OUT_OF_MEMORY = 9
+} ots_status;
+
+/* Stencil ids; names as the reference runners (opencl/<name>/). */
+typedef enum ots_stencil {
+  OTS_JACOBI_1D = 0,
+  OTS_JACOBI_1D_5PT = 1,
+  OTS_JACOBI_1D_7PT = 2,
+  OTS_JACOBI_2D = 3,
+  OTS_JACOBI_3D = 4,
+  OTS_POISSON_2D = 5,
+  OTS_POISSON_3D = 6,
+  OTS_GRADIENT_2D = 7,
+  OTS_GRADIENT_3D = 8,
+  OTS_FDTD_2D = 9,
+  OTS_RICIAN_DENOISE_2D = 10,
+  OTS_CDSC_TV_UPDATE_2D = 11,
+  OTS_CS_3D = 12,
+  OTS_NUM_STENCILS = 13
+} ots_stencil;
+
+/* Geometry derivation.  COMPAT truncates the problem to a multiple of the
+ * reference's sizeLCM and puts E on y in 3D, exactly as computeDerived does;
+ * NATIVE keeps the exact problem size (partial edge tiles) and puts E on z
+ * in 3D. */
+typedef enum ots_engine { OTS_ENGINE_NATIVE = 0, OTS_ENGINE_COMPAT = 1 } ots_engine;
+
+/* Kernel family.  TILE: overlapped time tile in every dimension (the
+ * reference scheme).  STREAM: overlapped in x/y, streamed along z with all T
+ * time levels in flight (3D star stencils).  PLAIN: one time step per launch
+ * (the comparator).  AUTO picks STREAM where available in 3D, else TILE. */
+typedef enum ots_kernel {
+  OTS_KERNEL_AUTO = 0,
+  OTS_KERNEL_TILE = 1,
+  OTS_KERNEL_STREAM = 2,
+  OTS_KERNEL_PLAIN = 3
+} ots_kernel;
+
+/* Arithmetic variant where the reference and the benchmark definition
+ * differ.  BASELINE: jacobi-3d weight 1/7; Poisson as a Jacobi sweep with RHS
+ * f and h^2 (5-/7-point); FDTD with the standard Hz sign and the Ey row-0
+ * source.  REF: the reference kernels' arithmetic (0.143f; 8c-sum8 and
+ * 26c-sum26; +Ey in the Hz update, no source). */
+typedef enum ots_variant { OTS_VARIANT_BASELINE = 0, OTS_VARIANT_REF = 1 } ots_variant;
+
+typedef struct ots_params {
+  int32_t stencil;             /* ots_stencil */
+  int32_t problem_size;        /* -n/--problem-size */
+  int32_t time_steps;          /* -t/--time-steps */
+  int32_t time_tile;           /* -s/--time-tile-size (T) */
+  int32_t block_x;             /* -x/--block-size-x (threads) */
+  int32_t block_y;             /* -y/--block-size-y */
+  int32_t block_z;             /* -z/--block-size-z */
+  int32_t elements_per_thread; /* -e/--elements-per-thread (E) */
+  int32_t engine;              /* ots_engine */
+  int32_t kernel;              /* ots_kernel */
+  int32_t variant;             /* ots_variant */
+  int32_t phase_limit;         /* -p/--phase-limit: 0 full, 1/2/3 partial kernels */
+  float coef;                  /* averaging weight; 0 = the stencil's default */
+  float h2;                    /* Poisson h^2; 0 = 1/(real_size-1)^2 */
+  int32_t device;              /* CUDA device ordinal */
+  int32_t reserved[7];         /* must be zero */
+} ots_params;
+
+/* Derived values: the reference's GeneratorParams fields plus what the
+ * chosen kernel actually launches. */
+typedef struct ots_geometry {
+  int32_t dims;
+  int32_t radius;              /* true per-step dependence radius */
+  int32_t num_fields;          /* evolving fields (ping-ponged) */
+  int32_t num_aux;             /* read-only fields */
+  int32_t padding;             /* host-layout ring width */
+  int32_t padded_size;         /* host-layout P */
+  int32_t real_size;           /* interior cells per axis */
+  int32_t size_lcm;
+  int32_t comps[3];            /* cells computed per CTA (incl. halo) */
+  int32_t real_per_block[3];   /* interior cells written per CTA */
+  int32_t num_blocks[3];       /* grid */
+  int32_t shared_size[3];      /* reference sharedSize{X,Y,Z} */
+  int32_t threads[3];          /* CTA shape launched */
+  int32_t kernel;              /* resolved ots_kernel */
+  int32_t e_axis;              /* axis E multiplies: 0 x, 1 y, 2 z */
+  int32_t launches;            /* ceil(time_steps / T) */
+  int32_t registers;           /* per thread, from cudaFuncGetAttributes */
+  int64_t shared_bytes;        /* dynamic shared memory per CTA */
+  int64_t interior_points;     /* real_size^dims */
+  double flops_per_point;      /* the reference's per-point constant */
+  double useful_ratio;         /* reference "Useful Ratio" */
+  float coef;                  /* averaging weight in effect */
+  float h2;                    /* Poisson h^2 in effect */
+} ots_geometry;
+
+typedef struct ots_timing {
+  double event_ms;             /* cudaEvent: first launch start -> last end */
+  double wall_s;               /* host wall clock around launch + sync */
+  int32_t launches;
+  int32_t steps;
+} ots_timing;
+
+typedef struct ots_plan ots_plan;
+
+/* ---- errors / device ------------------------------------------------- */
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* ots_last_error(void);
+const char* ots_status_string(ots_status s);
+
+/* Device name, SM count, shared memory per block (opt-in), global memory. */
+ots_status ots_device_info(int32_t device, char* name, size_t name_len, int32_t* sm_count,
+                           int64_t* smem_per_block, int64_t* global_mem);
+
+/* ---- stencil metadata -------------------------------------------------- */
+
+const char* ots_stencil_name(int32_t stencil);
+int32_t ots_stencil_from_name(const char* name); /* -1 if unknown */
+int32_t ots_stencil_dims(int32_t stencil);
+int32_t ots_stencil_num_fields(int32_t stencil);
+int32_t ots_stencil_num_aux(int32_t stencil);
+
+/* Fill P^d host arrays (state fields then aux fields, as the reference
+ * interleaves them per cell) with srand(seed); rand()/(RAND_MAX+1.0f) over
+ * the interior, zero on the ring (opencl/poisson-2d/poisson-2d.cpp:611-621). */
+ots_status ots_fill_reference(int32_t dims, int32_t padded_size, int32_t padding,
+                              int32_t real_size, uint32_t seed, float* const* fields,
+                              int32_t num_fields);
+
+/* ---- plans -------------------------------------------------------------- */
+
+/* Derive the geometry, pick and validate the kernel instantiation, allocate
+ * device buffers.  Replaces GeneratorParams::computeDerived + generate() +
+ * program build (opencl/jacobi-2d/jacobi-2d.cpp:84-126, 162-173, 741-780). */
+ots_status ots_plan_create(const ots_params* params, ots_plan** out);
+void ots_plan_destroy(ots_plan* plan);
+ots_status ots_plan_geometry(const ots_plan* plan, ots_geometry* out);
+
+/* Derive the geometry without allocating (what the reference prints before
+ * running).  Same validation as ots_plan_create. */
+ots_status ots_derive_geometry(const ots_params* params, ots_geometry* out);
+
+/* Copy host fields (reference layout, P^d each) into the plan.  `state` has
+ * num_fields arrays, `aux` num_aux arrays (may be NULL when num_aux == 0).
+ * Replaces the two enqueueWriteBuffer calls (jacobi-2d.cpp:874-886). */
+ots_status ots_upload(ots_plan* plan, const float* const* state, const float* const* aux);
+
+/* Same, from dense interior arrays (real_size^dims floats, no ring). */
+ots_status ots_upload_interior(ots_plan* plan, const float* const* state,
+                               const float* const* aux);
+
+/* Run time_steps steps: ceil(S/T) launches ping-ponging the state buffers
+ * (jacobi-2d.cpp:905-931).  `kernel` overrides the plan's kernel family for
+ * this run (OTS_KERNEL_AUTO keeps it).  The state advances in place, so a
+ * second call continues from the first call's result.  `timing` may be NULL. */
+ots_status ots_run(ots_plan* plan, int32_t kernel, ots_timing* timing);
+
+/* Enqueue the run on the plan's stream and return without synchronising
+ * (for CUDA-graph capture and timed loops); ots_sync waits for it. */
+ots_status ots_run_async(ots_plan* plan, int32_t kernel);
+ots_status ots_sync(ots_plan* plan);
+
+/* Copy the current state back (reference layout / dense interior);
+ * replaces enqueueReadBuffer(*inputBuffer) (jacobi-2d.cpp:952-954). */
+ots_status ots_download(ots_plan* plan, float* const* state);
+ots_status ots_download_interior(ots_plan* plan, float* const* state);
+
+/* Report the reference runner's key/value lines (printProgramParameters and
+ * the per-stencil model constants, jacobi-2d.cpp:1029-1037) through `kv`. */
+typedef void (*ots_kv_fn)(const char* key, const char* value, void* user);
+ots_status ots_describe(const ots_plan* plan, ots_kv_fn kv, void* user);
+
+/* Device pointers of the plan's current state / aux buffers (dense interior
+ * layout, x fastest), and its stream, for callers that keep data on the
+ * GPU between runs. */
+ots_status ots_plan_device_state(const ots_plan* plan, int32_t field, float** device_ptr);
+ots_status ots_plan_device_aux(const ots_plan* plan, int32_t field, float** device_ptr);
+ots_status ots_plan_stream(const ots_plan* plan, void** cuda_stream);
+
+/* Page-lock a caller's host buffer so uploads/downloads run as async DMA. */
+ots_status ots_host_register(void* ptr, size_t bytes);
+ots_status ots_host_unregister(void* ptr);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OTS_H */

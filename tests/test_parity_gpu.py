@@ -1,0 +1,233 @@
+"""GPU parity: every stencil and kernel family through the C ABI against the
+CPU oracle on identical seeded inputs.
+
+Linear stencils (the Jacobi family, both Poisson variants, both FDTD
+variants) must match bit for bit: the library is built with -fmad=false and
+keeps the oracle's operand order.  Stencils with a 1/sqrt term use the GPU
+rsqrt (as the reference kernels do) against 1/sqrt on the CPU; their
+tolerance is stated per stencil below.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import ots
+
+EXACT = {"jacobi-1d", "jacobi-1d-5pt", "jacobi-1d-7pt", "jacobi-2d", "jacobi-3d", "poisson-2d",
+         "poisson-3d", "fdtd-2d"}
+# max |gpu - cpu| / max(|cpu|, 1) after the step counts used here
+RTOL = {"gradient-2d": 2e-6, "gradient-3d": 2e-6, "rician-denoise-2d": 2e-5,
+        "cdsc-tv-update-2d": 2e-5, "cs-3d": 2e-5}
+
+
+def inputs(plan, seed):
+    state, aux = plan.fill_reference(seed=seed)
+    if plan.stencil in ("poisson-2d", "poisson-3d"):
+        aux = [np.where(a != 0, 2.0 * a - 1.0, 0.0).astype(np.float32) for a in aux]
+    return state, aux
+
+
+def run_and_check(stencil, n, steps, seed=123456, **kw):
+    with ots.Plan(stencil, n, steps, device=0, **kw) as plan:
+        g = plan.geometry
+        state, aux = inputs(plan, seed)
+        plan.upload(state, aux)
+        plan.run()
+        got = plan.download()
+        want = O.sweep_f32(stencil, state, aux=aux, steps=steps, lo=g.padding,
+                           hi=g.padding + g.real_size, variant=plan.params.variant,
+                           coef=g.coef, h2=g.h2)
+        for f, (a, b) in enumerate(zip(got, want)):
+            if stencil in EXACT:
+                bad = np.count_nonzero(a.view(np.uint32) != b.view(np.uint32))
+                assert bad == 0, "%s field %d: %d cells differ (max |d| %g)" % (
+                    stencil, f, bad, float(np.max(np.abs(a - b))))
+            else:
+                err = float(np.max(np.abs(a.astype(np.float64) - b) / np.maximum(np.abs(b), 1.0)))
+                assert err <= RTOL[stencil], "%s field %d: rel err %g" % (stencil, f, err)
+        return plan.geometry
+
+
+# (stencil, n, steps, T, bx, by, bz, E)
+TILE_CASES = [
+    ("jacobi-1d", 1000, 9, 3, 64, 1, 1, 4),
+    ("jacobi-1d", 777, 5, 1, 32, 1, 1, 1),
+    ("jacobi-1d-5pt", 1003, 10, 4, 128, 1, 1, 2),
+    ("jacobi-1d-7pt", 999, 7, 3, 64, 1, 1, 3),
+    ("jacobi-2d", 67, 9, 4, 16, 16, 1, 1),
+    ("jacobi-2d", 100, 64, 8, 32, 8, 1, 4),
+    ("jacobi-2d", 33, 5, 2, 16, 4, 1, 12),
+    ("poisson-2d", 71, 8, 3, 32, 8, 1, 2),
+    ("gradient-2d", 61, 6, 3, 16, 8, 1, 3),
+    ("fdtd-2d", 58, 11, 4, 32, 8, 1, 2),
+    ("fdtd-2d", 40, 3, 1, 16, 16, 1, 1),
+    ("rician-denoise-2d", 53, 5, 2, 32, 8, 1, 4),
+    ("cdsc-tv-update-2d", 49, 6, 3, 16, 16, 1, 2),
+    ("jacobi-3d", 37, 7, 3, 16, 8, 4, 4),
+    ("jacobi-3d", 20, 4, 1, 8, 8, 8, 1),
+    ("poisson-3d", 29, 5, 2, 16, 8, 2, 4),
+    ("gradient-3d", 27, 4, 2, 16, 4, 2, 4),
+    ("cs-3d", 25, 5, 2, 16, 8, 2, 3),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", TILE_CASES, ids=lambda c: "%s-n%d-T%d-E%d" % (c[0], c[1], c[3], c[7]))
+def test_tile_kernel_matches_oracle(case):
+    st, n, steps, T, bx, by, bz, E = case
+    run_and_check(st, n, steps, T=T, bx=bx, by=by, bz=bz, E=E, kernel="tile")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("st", ots.STENCILS)
+def test_plain_kernel_matches_oracle(st):
+    d = O.dims(st)
+    n = {1: 900, 2: 45, 3: 22}[d]
+    run_and_check(st, n, 5, kernel="plain")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("st", ["jacobi-2d", "poisson-2d", "gradient-2d", "fdtd-2d", "jacobi-3d",
+                                "poisson-3d", "cs-3d", "jacobi-1d-5pt"])
+def test_reference_variant_and_compat_engine(st):
+    d = O.dims(st)
+    if d == 1:
+        kw = dict(n=500, T=2, bx=64, by=1, bz=1, E=2)
+    elif d == 2:
+        kw = dict(n=70, T=3, bx=16, by=8, bz=1, E=2)
+    else:
+        kw = dict(n=30, T=1, bx=8, by=4, bz=4, E=2)
+    steps = 6 if st not in ("poisson-2d", "poisson-3d") else 4
+    g = run_and_check(st, kw.pop("n"), steps, engine=ots.ENGINE_COMPAT,
+                      variant=ots.VARIANT_REF, kernel="tile", **kw)
+    assert g.real_size % g.size_lcm == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("st", ["jacobi-3d", "poisson-3d", "gradient-3d"])
+@pytest.mark.parametrize("T", [1, 2, 3, 4, 5, 8])
+@pytest.mark.parametrize("E", [1, 2, 4])
+def test_stream_kernel_matches_oracle(st, T, E):
+    by = {1: 16, 2: 8, 4: 6}[E] if T < 5 else {1: 24, 2: 12, 4: 6}[E]
+    run_and_check(st, 41, 2 * T + 1, T=T, bx=16, by=by, bz=1, E=E, kernel="stream")
+
+
+@pytest.mark.gpu
+def test_stream_kernel_partial_tiles_and_segments():
+    # n not a multiple of the tile interior, more steps than one launch
+    run_and_check("jacobi-3d", 133, 10, T=4, bx=32, by=6, bz=1, E=4, kernel="stream")
+    run_and_check("jacobi-3d", 64, 13, T=3, bx=8, by=16, bz=1, E=2, kernel="stream")
+
+
+@pytest.mark.gpu
+def test_steps_zero_and_shallow_last_launch():
+    for steps in (0, 1, 5):
+        run_and_check("jacobi-2d", 50, steps, T=4, bx=16, by=16, E=1, kernel="tile")
+        run_and_check("jacobi-3d", 30, steps, T=4, bx=16, by=8, E=2, kernel="stream")
+
+
+@pytest.mark.gpu
+def test_repeated_runs_are_deterministic_and_continue():
+    with ots.Plan("jacobi-3d", 48, 6, T=3, bx=16, by=8, bz=1, E=2, kernel="stream") as plan:
+        state, _ = plan.fill_reference(seed=3)
+        plan.upload(state)
+        plan.run()
+        plan.run()  # second call continues from the first call's result
+        a = plan.download()[0]
+        plan.upload(state)
+        plan.run()
+        plan.run()
+        b = plan.download()[0]
+        g = plan.geometry
+        want = O.sweep_f32("jacobi-3d", state, steps=12, lo=g.padding, hi=g.padding + g.real_size,
+                           coef=g.coef)[0]
+    assert np.array_equal(a, b) and np.array_equal(a, want)
+
+
+@pytest.mark.gpu
+def test_kernel_families_agree_bitwise_on_one_plan():
+    with ots.Plan("poisson-3d", 52, 9, T=3, bx=16, by=8, bz=1, E=2, kernel="stream") as plan:
+        state, aux = inputs(plan, 11)
+        outs = []
+        for k in ("stream", "plain"):
+            plan.upload(state, aux)
+            plan.run(k)
+            outs.append(plan.download()[0])
+    assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_interior_upload_download_roundtrip():
+    with ots.Plan("fdtd-2d", 37, 3, T=2, bx=16, by=8, E=1, kernel="tile") as plan:
+        state, _ = plan.fill_reference(seed=8)
+        g = plan.geometry
+        inner = [np.ascontiguousarray(s[g.padding:g.padding + g.real_size,
+                                        g.padding:g.padding + g.real_size]) for s in state]
+        plan.upload_interior(inner)
+        plan.run()
+        a = plan.download_interior()
+        plan.upload(state)
+        plan.run()
+        b = plan.download()
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y[g.padding:g.padding + g.real_size,
+                                       g.padding:g.padding + g.real_size])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("limit", [1, 2, 3])
+def test_phase_limited_kernels_run(limit):
+    with ots.Plan("jacobi-2d", 64, 8, T=4, bx=16, by=16, E=1, kernel="tile",
+                  phase_limit=limit) as plan:
+        state, _ = plan.fill_reference()
+        plan.upload(state)
+        t = plan.run()
+        assert t.launches == 2
+
+
+@pytest.mark.gpu
+def test_errors_are_statuses_not_crashes():
+    with pytest.raises(ots.OtsError) as ei:
+        ots.Plan("jacobi-3d", 64, 4, T=4, bx=64, by=64, bz=1, E=4, kernel="stream")
+    assert ei.value.status_name in ("BLOCK_TOO_LARGE", "UNSUPPORTED", "SMEM_TOO_LARGE")
+    with pytest.raises(ots.OtsError) as ei:
+        ots.Plan("cs-3d", 32, 4, T=2, bx=16, by=8, bz=1, E=2, kernel="stream")
+    assert ei.value.status_name == "UNSUPPORTED"
+    with pytest.raises(ots.OtsError) as ei:
+        ots.Plan("jacobi-2d", 64, 4, T=2, bx=64, by=32, E=1, kernel="tile")
+    assert ei.value.status_name == "BLOCK_TOO_LARGE"
+    with pytest.raises(ots.OtsError) as ei:
+        ots.Plan("jacobi-2d", 64, 4, device=999)
+    assert ei.value.status_name == "INVALID_ARGUMENT"
+
+
+@pytest.mark.gpu
+def test_full_size_jacobi_3d_tiled_equals_plain_and_fp64_error():
+    """512^3 x 100 steps (the headline workload): the z-streamed time tile and
+    the plain one-step kernel give identical bits (size-independent property),
+    and the result's max relative error against an FP64 sweep of a 96^3 cut
+    with the same boundary stays within 1e-5."""
+    n, steps = 512, 100
+    with ots.Plan("jacobi-3d", n, steps, T=4, bx=32, by=8, bz=1, E=4, kernel="stream") as plan:
+        state, _ = plan.fill_reference(seed=123456)
+        plan.upload(state)
+        plan.run("stream")
+        a = plan.download_interior()[0]
+        plan.upload(state)
+        plan.run("plain")
+        b = plan.download_interior()[0]
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert np.isfinite(a).all() and 0.0 < float(a.mean()) < 1.0
+    # FP64 error on a smaller cube of the same workload shape
+    m = 96
+    with ots.Plan("jacobi-3d", m, steps, T=4, bx=32, by=8, bz=1, E=4, kernel="stream") as plan:
+        state, _ = plan.fill_reference(seed=123456)
+        plan.upload(state)
+        plan.run()
+        got = plan.download()[0]
+        g = plan.geometry
+    O.set_threads(8)
+    ref64 = O.sweep_f64("jacobi-3d", state, steps=steps, lo=g.padding, hi=g.padding + m,
+                        coef=g.coef)[0]
+    mr, rms = O.error_vs_f64(got, ref64, g.padding, g.padding + m, floor=1e-6)
+    assert mr <= 1e-5, mr
