@@ -239,6 +239,8 @@ def main():
     g = plan.geometry
     state, aux = plan.fill_reference(seed=123456 + rank)
     plan.upload(state, aux)
+    sl = tuple(slice(g.padding, g.padding + g.real_size) for _ in range(g.dims))
+    inner = ([np.ascontiguousarray(a[sl]) for a in state], [np.ascontiguousarray(a[sl]) for a in aux])
     stream = torch.cuda.ExternalStream(plan.stream_ptr(), device=local)
     launches_per_step = g.launches
 
@@ -278,7 +280,7 @@ def main():
     try:
         p1 = ots.Plan(STENCIL, N, STEPS, device=local, kernel="stream", T=1, bx=cfg["bx"],
                       by=cfg["by"], bz=1, E=cfg["E"])
-        p1.upload(state, aux)
+        p1.upload_interior(*inner)
         s1 = torch.cuda.ExternalStream(p1.stream_ptr(), device=local)
         for _ in range(2):
             p1.run_async()

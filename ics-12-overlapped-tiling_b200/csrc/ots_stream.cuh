@@ -109,9 +109,16 @@ struct StreamGeom {
   static constexpr int HY = T;
 };
 
+// Floats between consecutive shared plane buffers: the plane rounded up to
+// 128 bytes, because a TMA tensor copy needs a 128-byte aligned shared
+// destination (every ring stage is one).
+__host__ __device__ inline int stream_plane_stride(int TX, int TY) {
+  return (TX * TY + 31) / 32 * 32;
+}
+
 // Shared bytes: ring + (T-1) double-buffered exchange planes + mbarriers.
 __host__ __device__ inline size_t stream_smem_bytes(int T, int TX, int TY) {
-  size_t plane = (size_t)TX * TY * sizeof(float);
+  size_t plane = (size_t)stream_plane_stride(TX, TY) * sizeof(float);
   return (size_t)kStreamStages * plane + (size_t)(T > 1 ? T - 1 : 0) * 2 * plane + 128;
 }
 
@@ -130,7 +137,8 @@ __global__ void __launch_bounds__(StreamThreads<E>::kMax, 1)
   constexpr int NST = kStreamStages, LA = kStreamStages - 3;
   extern __shared__ __align__(128) float smem[];
   const int BX = blockDim.x, BY = blockDim.y;
-  const int TX = V * BX, TY = E * BY, PL = TX * TY;
+  const int TX = V * BX, TY = E * BY;
+  const int PL = stream_plane_stride(TX, TY);  // buffer stride; the box is TX*TY
   const int rpbx = TX - 2 * HX, rpby = TY - 2 * HY;
   const int tx0 = blockIdx.x * rpbx - HX;  // multiple of 4
   const int ty0 = blockIdx.y * rpby - HY;
@@ -150,7 +158,7 @@ __global__ void __launch_bounds__(StreamThreads<E>::kMax, 1)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   __syncthreads();
-  const unsigned plane_bytes = (unsigned)PL * sizeof(float);
+  const unsigned plane_bytes = (unsigned)(TX * TY) * sizeof(float);
   if (tid == 0) {
     for (int j = 0; j < LA && kb + j <= ke; ++j) {
       mbar_arrive_expect_tx(&bars[j % NST], plane_bytes);

@@ -244,14 +244,29 @@ class Plan:
                               g.num_fields + g.num_aux)
         return arrs[:g.num_fields], arrs[g.num_fields:]
 
+    @property
+    def interior_shape(self):
+        return (self.geometry.real_size,) * self.geometry.dims
+
+    def _checked(self, arrays, count, shape, what):
+        arrs = [np.ascontiguousarray(a, np.float32) for a in arrays]
+        if len(arrs) != count:
+            raise ValueError("%s: expected %d arrays, got %d" % (what, count, len(arrs)))
+        for a in arrs:
+            if a.shape != shape:
+                raise ValueError("%s: array shape %s, plan needs %s" % (what, a.shape, shape))
+        return arrs
+
     def upload(self, state, aux=()):
-        st = [np.ascontiguousarray(a, np.float32) for a in state]
-        ax = [np.ascontiguousarray(a, np.float32) for a in aux]
+        g = self.geometry
+        st = self._checked(state, g.num_fields, self.padded_shape, "state")
+        ax = self._checked(aux, g.num_aux, self.padded_shape, "aux")
         check(lib().ots_upload(self.handle, _fptrs(st), _fptrs(ax) if ax else None))
 
     def upload_interior(self, state, aux=()):
-        st = [np.ascontiguousarray(a, np.float32) for a in state]
-        ax = [np.ascontiguousarray(a, np.float32) for a in aux]
+        g = self.geometry
+        st = self._checked(state, g.num_fields, self.interior_shape, "state")
+        ax = self._checked(aux, g.num_aux, self.interior_shape, "aux")
         check(lib().ots_upload_interior(self.handle, _fptrs(st), _fptrs(ax) if ax else None))
 
     def run(self, kernel=KERNEL_AUTO):
@@ -271,13 +286,23 @@ class Plan:
         g = self.geometry
         if out is None:
             out = [np.zeros(self.padded_shape, np.float32) for _ in range(g.num_fields)]
+        for a in out:
+            if a.shape != self.padded_shape or a.dtype != np.float32 or not a.flags.c_contiguous:
+                raise ValueError("download: need C-contiguous float32 %s" % (self.padded_shape,))
+        if len(out) != g.num_fields:
+            raise ValueError("download: expected %d arrays" % g.num_fields)
         check(lib().ots_download(self.handle, _fptrs(out)))
         return out
 
     def download_interior(self, out=None):
         g = self.geometry
         if out is None:
-            out = [np.zeros((g.real_size,) * g.dims, np.float32) for _ in range(g.num_fields)]
+            out = [np.zeros(self.interior_shape, np.float32) for _ in range(g.num_fields)]
+        for a in out:
+            if a.shape != self.interior_shape or a.dtype != np.float32 or not a.flags.c_contiguous:
+                raise ValueError("download: need C-contiguous float32 %s" % (self.interior_shape,))
+        if len(out) != g.num_fields:
+            raise ValueError("download: expected %d arrays" % g.num_fields)
         check(lib().ots_download_interior(self.handle, _fptrs(out)))
         return out
 

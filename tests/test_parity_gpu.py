@@ -15,8 +15,10 @@ import ots
 
 EXACT = {"jacobi-1d", "jacobi-1d-5pt", "jacobi-1d-7pt", "jacobi-2d", "jacobi-3d", "poisson-2d",
          "poisson-3d", "fdtd-2d"}
-# max |gpu - cpu| / max(|cpu|, 1) after the step counts used here
-RTOL = {"gradient-2d": 2e-6, "gradient-3d": 2e-6, "rician-denoise-2d": 2e-5,
+# max |gpu - cpu| / max(|cpu|, 1) after the step counts used here.  rsqrtf
+# is within 2 ulp per call; gradient's 1/sqrt(1e-4 + sum d^2) amplifies that
+# by its sensitivity to the differences d (measured 2.2e-5 on B200).
+RTOL = {"gradient-2d": 1e-4, "gradient-3d": 1e-4, "rician-denoise-2d": 2e-5,
         "cdsc-tv-update-2d": 2e-5, "cs-3d": 2e-5}
 
 
