@@ -150,7 +150,7 @@ int main(int argc, char** argv) {
   p.kernel = OTS_KERNEL_AUTO;
   p.variant = -1;
   unsigned seed = 123456;  // srand(123456), opencl/jacobi-2d/jacobi-2d.cpp:561
-  bool verify = false, plain = false;
+  bool verify = false, plain = false, bx_set = false, by_set = false;
   std::string save_kernel, load_kernel;
 
   for (int i = 1; i < argc; ++i) {
@@ -174,8 +174,13 @@ int main(int argc, char** argv) {
       return 1;
     } else if (a == "-n" || a == "--problem-size") p.problem_size = atoi(next());
     else if (a == "-t" || a == "--time-steps") p.time_steps = atoi(next());
-    else if (a == "-x" || a == "--block-size-x") p.block_x = atoi(next());
-    else if (a == "-y" || a == "--block-size-y") p.block_y = atoi(next());
+    else if (a == "-x" || a == "--block-size-x") {
+      p.block_x = atoi(next());
+      bx_set = true;
+    } else if (a == "-y" || a == "--block-size-y") {
+      p.block_y = atoi(next());
+      by_set = true;
+    }
     else if (a == "-z" || a == "--block-size-z") p.block_z = atoi(next());
     else if (a == "-e" || a == "--elements-per-thread") p.elements_per_thread = atoi(next());
     else if (a == "-s" || a == "--time-tile-size") p.time_tile = atoi(next());
@@ -215,10 +220,10 @@ int main(int argc, char** argv) {
   const int dims = ots_stencil_dims(stencil);
   if (p.problem_size < 0) p.problem_size = dims == 3 ? 128 : (dims == 1 ? 1024 : 1024);
   if (p.block_z < 0) p.block_z = dims == 3 ? 8 : 1;
-  if (dims == 3 && p.block_x == 16 && p.block_y == 16) {
+  if (dims == 3) {
     // 3D runner defaults, opencl/jacobi-3d/jacobi-3d.cpp:486-523
-    p.block_x = 8;
-    p.block_y = 8;
+    if (!bx_set) p.block_x = 8;
+    if (!by_set) p.block_y = 8;
   }
   if (dims == 1) p.block_y = p.block_z = 1;
   if (dims == 2) p.block_z = 1;

@@ -330,7 +330,13 @@ ots_status derive_stream(const ots_plan* pl, int T, StreamCfg* c) {
   c->ty = c->E * c->by;
   c->rpbx = c->tx - 2 * hx;
   c->rpby = c->ty - 2 * hy;
-  const int maxthr = c->E >= 4 ? 256 : 512;
+  const int maxthr = T * c->E >= 8 ? 256 : 512;
+  if (c->bx != 8 && c->bx != 16 && c->bx != 32)
+    return fail(OTS_ERR_UNSUPPORTED, "stream kernel block x must be 8, 16 or 32 (got %d)", c->bx);
+  if ((c->bx * c->by) % 32 != 0)
+    return fail(OTS_ERR_UNSUPPORTED,
+                "stream kernel needs whole warps (block %d x %d is not a multiple of 32 threads)",
+                c->bx, c->by);
   if (c->bx * c->by > maxthr)
     return fail(OTS_ERR_BLOCK_TOO_LARGE, "Block dimensions are too large! (%d x %d > %d threads)",
                 c->bx, c->by, maxthr);

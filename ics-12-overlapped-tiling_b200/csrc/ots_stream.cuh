@@ -42,7 +42,7 @@ struct StreamParams {
   OpArgs op;
 };
 
-constexpr int kStreamStages = 5;  // ring depth; lookahead = stages - 3
+constexpr int kStreamStages = 4;  // ring depth; lookahead = stages - 2
 constexpr unsigned kWaitLimit = 1u << 24;
 constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s
 
@@ -122,35 +122,71 @@ __host__ __device__ inline size_t stream_smem_bytes(int T, int TX, int TY) {
   return (size_t)kStreamStages * plane + (size_t)(T > 1 ? T - 1 : 0) * 2 * plane + 128;
 }
 
-// Threads per CTA are capped so that E = 4 (16 cells per thread and level)
-// keeps its register rings without spilling.
-template <int E>
+// Threads per CTA are capped so that the register rings (3 planes of 4E
+// cells per level) stay in registers.
+template <int T, int E>
 struct StreamThreads {
-  static constexpr int kMax = E >= 4 ? 256 : 512;
+  static constexpr int kMax = (T * E >= 8) ? 256 : 512;
 };
 
+template <int N>
+struct Phase {
+  static constexpr int value = N;
+};
+
+// blockDim.x (threads along x) must be 8, 16 or 32: a warp then holds whole
+// rows of the tile, so every x neighbour a shuffle cannot reach (lane 0's
+// left, lane 31's right) is a tile-edge halo cell whose value is never used.
 template <class Op, int T, int E>
-__global__ void __launch_bounds__(StreamThreads<E>::kMax, 1)
-    stream_kernel(const __grid_constant__ CUtensorMap tmap, const StreamParams p) {
+__global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
+    stream_kernel(const __grid_constant__ CUtensorMap tmap,
+                  const __grid_constant__ StreamParams p) {
   constexpr int V = 4;
   constexpr int HX = StreamGeom<T>::HX, HY = StreamGeom<T>::HY;
-  constexpr int NST = kStreamStages, LA = kStreamStages - 3;
+  constexpr int NST = kStreamStages, LA = kStreamStages - 2;
   extern __shared__ __align__(128) float smem[];
   const int BX = blockDim.x, BY = blockDim.y;
   const int TX = V * BX, TY = E * BY;
-  const int PL = stream_plane_stride(TX, TY);  // buffer stride; the box is TX*TY
+  const int PL = stream_plane_stride(TX, TY);
   const int rpbx = TX - 2 * HX, rpby = TY - 2 * HY;
-  const int tx0 = blockIdx.x * rpbx - HX;  // multiple of 4
+  const int tx0 = blockIdx.x * rpbx - HX;  // multiple of 4 (TMA x alignment)
   const int ty0 = blockIdx.y * rpby - HY;
   const int zs = blockIdx.z * p.zseg;
-  int ze = zs + p.zseg;
-  if (ze > p.L.n2) ze = p.L.n2;
-  const int kb = zs - T, ke = ze + T - 1;
+  const int ze = min(zs + p.zseg, p.L.n2);
+  const int kb = zs - T, ke = ze + T - 1, nit = ke - kb + 1;
   const int tid = threadIdx.x + BX * threadIdx.y;
+  const int XB = NST * PL;  // exchange planes start (floats)
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + XB + (T > 1 ? (T - 1) * 2 * PL : 0));
+  const unsigned box_bytes = (unsigned)(TX * TY) * sizeof(float);
 
-  float* ring = smem;
-  float* xbuf = smem + NST * PL;  // [(T-1)][2][PL]
-  uint64_t* bars = reinterpret_cast<uint64_t*>(xbuf + (T > 1 ? (T - 1) * 2 * PL : 0));
+  // per-thread constant shared offsets (floats)
+  const int lx = V * threadIdx.x, ly = E * threadIdx.y;
+  const int o_top = (ly > 0 ? ly - 1 : 0) * TX + lx;          // clamped: tile-edge halo
+  const int o_bot = (ly + E < TY ? ly + E : TY - 1) * TX + lx;
+  const int o_row0 = ly * TX + lx;
+  const int gx = tx0 + lx, gy = ty0 + ly;
+  unsigned xyin = 0;
+#pragma unroll
+  for (int e = 0; e < E; ++e)
+#pragma unroll
+    for (int v = 0; v < V; ++v)
+      if ((unsigned)(gx + v) < (unsigned)p.L.n0 && (unsigned)(gy + e) < (unsigned)p.L.n1)
+        xyin |= 1u << (e * V + v);
+  const bool xyall = xyin == ((E * V >= 32) ? 0xFFFFFFFFu : ((1u << (E * V)) - 1u));
+  const bool wx = lx >= HX && lx < HX + rpbx;
+  float* const obase = p.out + (int64_t)gy * p.L.sy + gx;
+  const float* const abase = p.aux + (int64_t)gy * p.L.sy + gx;
+
+  // R[t][slot]: level t's (0 = input) three newest planes of own cells.
+  float R[T][3][E][V];
+#pragma unroll
+  for (int t = 0; t < T; ++t)
+#pragma unroll
+    for (int s = 0; s < 3; ++s)
+#pragma unroll
+      for (int e = 0; e < E; ++e)
+#pragma unroll
+        for (int v = 0; v < V; ++v) R[t][s][e][v] = 0.0f;
 
   if (tid == 0) {
     for (int s = 0; s < NST; ++s) mbar_init(&bars[s], 1);
@@ -158,109 +194,58 @@ __global__ void __launch_bounds__(StreamThreads<E>::kMax, 1)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   __syncthreads();
-  const unsigned plane_bytes = (unsigned)(TX * TY) * sizeof(float);
   if (tid == 0) {
-    for (int j = 0; j < LA && kb + j <= ke; ++j) {
-      mbar_arrive_expect_tx(&bars[j % NST], plane_bytes);
-      tma_load_3d(ring + (j % NST) * PL, &tmap, tx0, ty0, kb + j, &bars[j % NST]);
+    for (int j = 0; j < LA && j < nit; ++j) {
+      mbar_arrive_expect_tx(&bars[j], box_bytes);
+      tma_load_3d(smem + j * PL, &tmap, tx0, ty0, kb + j, &bars[j]);
     }
   }
 
-  // Own cells: x = 4*tx .. +3, rows y = E*ty .. +E-1 (tile coordinates).
-  const int lx = V * threadIdx.x, ly = E * threadIdx.y;
-  const int lft = lx > 0 ? lx - 1 : 0;            // clamped: tile-edge cells are halo
-  const int rgt = lx + V < TX ? lx + V : TX - 1;
-  const int top = ly > 0 ? ly - 1 : 0;
-  const int bot = ly + E < TY ? ly + E : TY - 1;
-  const int gx = tx0 + lx, gy = ty0 + ly;
-  unsigned xyin = 0;  // bit (e*4+v): cell inside the domain in x and y
-#pragma unroll
-  for (int e = 0; e < E; ++e)
-#pragma unroll
-    for (int v = 0; v < V; ++v)
-      if ((unsigned)(gx + v) < (unsigned)p.L.n0 && (unsigned)(gy + e) < (unsigned)p.L.n1)
-        xyin |= 1u << (e * V + v);
-  const bool wx = lx >= HX && lx < HX + rpbx;
-
-  float C[T > 1 ? T - 1 : 1][E][V];  // level t (1..T-1): plane k-1-t (centre for level t+1)
-  float P[T > 1 ? T - 1 : 1][E][V];  // level t: plane k-2-t
-#pragma unroll
-  for (int t = 0; t < (T > 1 ? T - 1 : 1); ++t)
-#pragma unroll
-    for (int e = 0; e < E; ++e)
-#pragma unroll
-      for (int v = 0; v < V; ++v) C[t][e][v] = P[t][e][v] = 0.0f;
-
-  for (int k = kb; k <= ke; ++k) {
-    const int r = k - kb;
-    const bool to = !mbar_wait_bounded(&bars[r % NST], (r / NST) & 1, p.err);
+  int fail_r = -1;
+  auto step = [&](auto ph, int r) -> bool {
+    constexpr int PH = decltype(ph)::value;
+    constexpr int SN = PH, SC = (PH + 2) % 3, SM = (PH + 1) % 3;  // newest, centre, z-1
+    const int k = kb + r;
+    const int st = r & (NST - 1);
+    const bool to = !mbar_wait_bounded(&bars[st], (r / NST) & 1, p.err);
     if (__syncthreads_or(to)) {
-      if (tid == 0) {
-        atomicOr(p.err, 1);
-        // drain this CTA's copies still in flight (bounded) before leaving
-        for (int j = k; j <= ke && j < k + LA; ++j) {
-          const int rj = j - kb;
-          mbar_wait_bounded(&bars[rj % NST], (rj / NST) & 1, p.err);
-        }
-      }
-      __syncthreads();
-      return;
+      fail_r = r;
+      return false;
     }
-    if (tid == 0 && k + LA <= ke) {
-      const int s = (r + LA) % NST;
-      mbar_arrive_expect_tx(&bars[s], plane_bytes);
-      tma_load_3d(ring + s * PL, &tmap, tx0, ty0, k + LA, &bars[s]);
+    if (tid == 0 && r + LA < nit) {
+      const int s2 = (r + LA) & (NST - 1);
+      mbar_arrive_expect_tx(&bars[s2], box_bytes);
+      tma_load_3d(smem + s2 * PL, &tmap, tx0, ty0, k + LA, &bars[s2]);
     }
-
-    float N[E][V];  // newest plane of the level below, handed upwards
+    // level 0: the input plane k into registers
+    const int pk = st * PL;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const float4 a = *reinterpret_cast<const float4*>(smem + pk + o_row0 + e * TX);
+      R[0][SN][e][0] = a.x; R[0][SN][e][1] = a.y; R[0][SN][e][2] = a.z; R[0][SN][e][3] = a.w;
+    }
+    const int pc0 = ((r + NST - 1) & (NST - 1)) * PL;   // input plane k-1 (level 1 centre)
+    const int xr = XB + ((r - 1) & 1) * PL;              // exchange planes of iteration r-1
+    const int xw = XB + (r & 1) * PL;                    // exchange planes of iteration r
 #pragma unroll
     for (int t = 1; t <= T; ++t) {
-      const int q = k - t;  // plane this level computes
-      // centre plane of level t-1 (its x/y neighbours live in shared memory)
-      const float* cp;
-      float cen[E][V], zm[E][V], zp[E][V];
-      if (t == 1) {
-        const float* pk = ring + (r % NST) * PL;            // plane k   (z+1)
-        const float* pc = ring + ((r + NST - 1) % NST) * PL;  // plane k-1 (centre)
-        const float* pm = ring + ((r + NST - 2) % NST) * PL;  // plane k-2 (z-1)
-        cp = pc;
-#pragma unroll
-        for (int e = 0; e < E; ++e) {
-          const float4 a = *reinterpret_cast<const float4*>(pk + (ly + e) * TX + lx);
-          const float4 b = *reinterpret_cast<const float4*>(pc + (ly + e) * TX + lx);
-          const float4 c = *reinterpret_cast<const float4*>(pm + (ly + e) * TX + lx);
-          zp[e][0] = a.x; zp[e][1] = a.y; zp[e][2] = a.z; zp[e][3] = a.w;
-          cen[e][0] = b.x; cen[e][1] = b.y; cen[e][2] = b.z; cen[e][3] = b.w;
-          zm[e][0] = c.x; zm[e][1] = c.y; zm[e][2] = c.z; zm[e][3] = c.w;
-        }
-      } else {
-        cp = xbuf + ((t - 2) * 2 + ((k - 1) & 1)) * PL;  // written by level t-1 last plane
-#pragma unroll
-        for (int e = 0; e < E; ++e)
-#pragma unroll
-          for (int v = 0; v < V; ++v) {
-            cen[e][v] = C[t - 2][e][v];
-            zm[e][v] = P[t - 2][e][v];
-            zp[e][v] = N[e][v];
-          }
-      }
+      const int q = k - t;
+      const int cp = (t == 1) ? pc0 : xr + (t - 2) * 2 * PL;
+      const float4 tv = *reinterpret_cast<const float4*>(smem + cp + o_top);
+      const float4 bv = *reinterpret_cast<const float4*>(smem + cp + o_bot);
       float lv[E], rv[E];
 #pragma unroll
       for (int e = 0; e < E; ++e) {
-        lv[e] = cp[(ly + e) * TX + lft];
-        rv[e] = cp[(ly + e) * TX + rgt];
+        lv[e] = __shfl_up_sync(0xffffffffu, R[t - 1][SC][e][V - 1], 1);
+        rv[e] = __shfl_down_sync(0xffffffffu, R[t - 1][SC][e][0], 1);
       }
-      const float4 tv = *reinterpret_cast<const float4*>(cp + top * TX + lx);
-      const float4 bv = *reinterpret_cast<const float4*>(cp + bot * TX + lx);
-      const float tvv[V] = {tv.x, tv.y, tv.z, tv.w};
-      const float bvv[V] = {bv.x, bv.y, bv.z, bv.w};
+      const bool zin = (unsigned)q < (unsigned)p.L.n2;
       float fa[E][V];
       if (Op::NA > 0) {
-        const bool zin = (unsigned)q < (unsigned)p.L.n2;
 #pragma unroll
         for (int e = 0; e < E; ++e) {
           const unsigned m = (xyin >> (e * V)) & 0xF;
-          const float* src = p.aux + (int64_t)q * p.L.sz + (int64_t)(gy + e) * p.L.sy + gx;
+          const float* src = abase + (int64_t)q * p.L.sz + (int64_t)e * p.L.sy;
           if (zin && m == 0xF) {
             const float4 f4 = __ldg(reinterpret_cast<const float4*>(src));
             fa[e][0] = f4.x; fa[e][1] = f4.y; fa[e][2] = f4.z; fa[e][3] = f4.w;
@@ -270,71 +255,79 @@ __global__ void __launch_bounds__(StreamThreads<E>::kMax, 1)
           }
         }
       }
-      const bool zin = (unsigned)q < (unsigned)p.L.n2;
+      const float tvv[V] = {tv.x, tv.y, tv.z, tv.w};
+      const float bvv[V] = {bv.x, bv.y, bv.z, bv.w};
       float out[E][V];
 #pragma unroll
       for (int e = 0; e < E; ++e)
 #pragma unroll
         for (int v = 0; v < V; ++v) {
-          const float xm = v > 0 ? cen[e][v - 1] : lv[e];
-          const float xp = v < V - 1 ? cen[e][v + 1] : rv[e];
-          const float ym = e > 0 ? cen[e - 1][v] : tvv[v];
-          const float yp = e < E - 1 ? cen[e + 1][v] : bvv[v];
-          float res = Op::star(xm, cen[e][v], xp, ym, yp, zm[e][v], zp[e][v],
-                               Op::NA > 0 ? fa[e][v] : 0.0f, p.op);
-          const bool in = zin && ((xyin >> (e * V + v)) & 1);
-          out[e][v] = in ? res : 0.0f;
+          const float xm = v > 0 ? R[t - 1][SC][e][v - 1] : lv[e];
+          const float xp = v < V - 1 ? R[t - 1][SC][e][v + 1] : rv[e];
+          const float ym = e > 0 ? R[t - 1][SC][e - 1][v] : tvv[v];
+          const float yp = e < E - 1 ? R[t - 1][SC][e + 1][v] : bvv[v];
+          out[e][v] = Op::star(xm, R[t - 1][SC][e][v], xp, ym, yp, R[t - 1][SM][e][v],
+                               R[t - 1][SN][e][v], Op::NA > 0 ? fa[e][v] : 0.0f, p.op);
         }
+      if (!(zin && xyall)) {  // domain edge: zero the cells outside
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+#pragma unroll
+          for (int v = 0; v < V; ++v)
+            if (!(zin && ((xyin >> (e * V + v)) & 1))) out[e][v] = 0.0f;
+      }
       if (t < T) {
-        float* xb = xbuf + ((t - 1) * 2 + (k & 1)) * PL;
-#pragma unroll
-        for (int e = 0; e < E; ++e)
-          *reinterpret_cast<float4*>(xb + (ly + e) * TX + lx) =
-              make_float4(out[e][0], out[e][1], out[e][2], out[e][3]);
-        if (t >= 2) {
-          // level t-1's registers have been consumed by this level: shift
-#pragma unroll
-          for (int e = 0; e < E; ++e)
-#pragma unroll
-            for (int v = 0; v < V; ++v) {
-              P[t - 2][e][v] = C[t - 2][e][v];
-              C[t - 2][e][v] = N[e][v];
-            }
-        }
+        // other warps need only this thread's first and last rows (y
+        // neighbours); x neighbours travel by shuffle
+        const int xb = xw + (t - 1) * 2 * PL;
+        *reinterpret_cast<float4*>(smem + xb + o_row0) =
+            make_float4(out[0][0], out[0][1], out[0][2], out[0][3]);
+        if (E > 1)
+          *reinterpret_cast<float4*>(smem + xb + o_row0 + (E - 1) * TX) =
+              make_float4(out[E - 1][0], out[E - 1][1], out[E - 1][2], out[E - 1][3]);
 #pragma unroll
         for (int e = 0; e < E; ++e)
 #pragma unroll
-          for (int v = 0; v < V; ++v) N[e][v] = out[e][v];
-      } else {
-        if (T >= 2) {
+          for (int v = 0; v < V; ++v) R[t][SN][e][v] = out[e][v];
+      } else if (q >= zs && q < ze && wx) {
+        float* dst = obase + (int64_t)q * p.L.sz;
 #pragma unroll
-          for (int e = 0; e < E; ++e)
+        for (int e = 0; e < E; ++e) {
+          const int yy = ly + e;
+          if (yy < HY || yy >= HY + rpby) continue;
+          const unsigned m = (xyin >> (e * V)) & 0xF;
+          if (m == 0xF) {
+            *reinterpret_cast<float4*>(dst + (int64_t)e * p.L.sy) =
+                make_float4(out[e][0], out[e][1], out[e][2], out[e][3]);
+          } else {
 #pragma unroll
-            for (int v = 0; v < V; ++v) {
-              P[T - 2][e][v] = C[T - 2][e][v];
-              C[T - 2][e][v] = N[e][v];
-            }
-        }
-        if (q >= zs && q < ze && wx) {
-#pragma unroll
-          for (int e = 0; e < E; ++e) {
-            const int yy = ly + e;
-            if (yy < HY || yy >= HY + rpby) continue;
-            const unsigned m = (xyin >> (e * V)) & 0xF;
-            if (m == 0) continue;
-            float* dst = p.out + (int64_t)q * p.L.sz + (int64_t)(gy + e) * p.L.sy + gx;
-            if (m == 0xF) {
-              *reinterpret_cast<float4*>(dst) =
-                  make_float4(out[e][0], out[e][1], out[e][2], out[e][3]);
-            } else {
-#pragma unroll
-              for (int v = 0; v < V; ++v)
-                if ((m >> v) & 1) dst[v] = out[e][v];
-            }
+            for (int v = 0; v < V; ++v)
+              if ((m >> v) & 1) dst[(int64_t)e * p.L.sy + v] = out[e][v];
           }
         }
       }
     }
+    return true;
+  };
+
+  bool ok = true;
+  int r = 0;
+  for (; r + 2 < nit && ok; r += 3) {
+    ok = step(Phase<0>{}, r);
+    if (ok) ok = step(Phase<1>{}, r + 1);
+    if (ok) ok = step(Phase<2>{}, r + 2);
+  }
+  if (ok && r < nit) ok = step(Phase<0>{}, r++);
+  if (ok && r < nit) ok = step(Phase<1>{}, r++);
+  if (!ok) {
+    if (tid == 0) {
+      atomicOr(p.err, 1);
+      // drain this CTA's copies still in flight (bounded) before leaving:
+      // planes fail_r .. fail_r + LA - 1 were issued
+      for (int j = fail_r; j < nit && j < fail_r + LA; ++j)
+        mbar_wait_bounded(&bars[j & (NST - 1)], (j / NST) & 1, p.err);
+    }
+    __syncthreads();
   }
 }
 

@@ -110,15 +110,19 @@ def test_reference_variant_and_compat_engine(st):
 @pytest.mark.parametrize("T", [1, 2, 3, 4, 5, 8])
 @pytest.mark.parametrize("E", [1, 2, 4])
 def test_stream_kernel_matches_oracle(st, T, E):
-    by = {1: 16, 2: 8, 4: 6}[E] if T < 5 else {1: 24, 2: 12, 4: 6}[E]
-    run_and_check(st, 41, 2 * T + 1, T=T, bx=16, by=by, bz=1, E=E, kernel="stream")
+    if T < 5:
+        bx, by = {1: (16, 16), 2: (16, 8), 4: (16, 6)}[E]
+    else:
+        bx, by = {1: (8, 24), 2: (16, 12), 4: (16, 6)}[E]
+    run_and_check(st, 41, 2 * T + 1, T=T, bx=bx, by=by, bz=1, E=E, kernel="stream")
 
 
 @pytest.mark.gpu
 def test_stream_kernel_partial_tiles_and_segments():
     # n not a multiple of the tile interior, more steps than one launch
-    run_and_check("jacobi-3d", 133, 10, T=4, bx=32, by=6, bz=1, E=4, kernel="stream")
+    run_and_check("jacobi-3d", 133, 10, T=4, bx=32, by=6, bz=1, E=2, kernel="stream")
     run_and_check("jacobi-3d", 64, 13, T=3, bx=8, by=16, bz=1, E=2, kernel="stream")
+    run_and_check("jacobi-3d", 150, 9, T=2, bx=32, by=4, bz=1, E=4, kernel="stream")
 
 
 @pytest.mark.gpu
@@ -190,7 +194,7 @@ def test_phase_limited_kernels_run(limit):
 @pytest.mark.gpu
 def test_errors_are_statuses_not_crashes():
     with pytest.raises(ots.OtsError) as ei:
-        ots.Plan("jacobi-3d", 64, 4, T=4, bx=64, by=64, bz=1, E=4, kernel="stream")
+        ots.Plan("jacobi-3d", 64, 4, T=4, bx=32, by=64, bz=1, E=4, kernel="stream")
     assert ei.value.status_name in ("BLOCK_TOO_LARGE", "UNSUPPORTED", "SMEM_TOO_LARGE")
     with pytest.raises(ots.OtsError) as ei:
         ots.Plan("cs-3d", 32, 4, T=2, bx=16, by=8, bz=1, E=2, kernel="stream")
@@ -210,7 +214,7 @@ def test_full_size_jacobi_3d_tiled_equals_plain_and_fp64_error():
     and the result's max relative error against an FP64 sweep of a 96^3 cut
     with the same boundary stays within 1e-5."""
     n, steps = 512, 100
-    with ots.Plan("jacobi-3d", n, steps, T=4, bx=32, by=8, bz=1, E=4, kernel="stream") as plan:
+    with ots.Plan("jacobi-3d", n, steps, T=4, bx=32, by=8, bz=1, E=2, kernel="stream") as plan:
         state, _ = plan.fill_reference(seed=123456)
         plan.upload(state)
         plan.run("stream")
@@ -222,7 +226,7 @@ def test_full_size_jacobi_3d_tiled_equals_plain_and_fp64_error():
     assert np.isfinite(a).all() and 0.0 < float(a.mean()) < 1.0
     # FP64 error on a smaller cube of the same workload shape
     m = 96
-    with ots.Plan("jacobi-3d", m, steps, T=4, bx=32, by=8, bz=1, E=4, kernel="stream") as plan:
+    with ots.Plan("jacobi-3d", m, steps, T=4, bx=32, by=8, bz=1, E=2, kernel="stream") as plan:
         state, _ = plan.fill_reference(seed=123456)
         plan.upload(state)
         plan.run()
