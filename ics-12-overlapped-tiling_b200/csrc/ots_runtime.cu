@@ -96,6 +96,11 @@ const StencilInfo kInfo[OTS_NUM_STENCILS] = {
 };
 
 thread_local std::string g_last_error;
+}  // namespace
+
+void ots_set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
+
+namespace {
 
 ots_status fail(ots_status s, const char* fmt, ...) {
   char buf[1024];
@@ -161,6 +166,9 @@ struct StreamCfg {
   int T = 0, E = 0, eidx = 0, bx = 0, by = 0;
   int tx = 0, ty = 0, rpbx = 0, rpby = 0, zseg = 0;
   int nbx = 0, nby = 0, nbz = 0;
+  int grid = 0;            // persistent CTAs launched
+  int64_t work = 0;        // output tile-planes
+  int64_t chunk = 0;       // tile-planes per CTA
   size_t smem = 0;
 };
 
@@ -360,6 +368,10 @@ ots_status derive_stream(const ots_plan* pl, int T, StreamCfg* c) {
     int b = 0;
     if (pl->K->stream_occ[T][eidx](&b, c->bx * c->by, c->smem) == cudaSuccess && b > 0) per_sm = b;
   }
+  // Grid schedule: (tile, z segment) with tiles fastest.  The segment count
+  // trades the T-plane pipeline fill of each segment against whole waves of
+  // resident CTAs.
+  const int64_t work = (int64_t)c->nbx * c->nby * n;
   const int slots = std::max(1, pl->sm_count) * per_sm;
   const int xy = c->nbx * c->nby;
   double best = 1e300;
@@ -376,6 +388,9 @@ ots_status derive_stream(const ots_plan* pl, int T, StreamCfg* c) {
   }
   c->zseg = best_seg;
   c->nbz = ceil_div(n, c->zseg);
+  c->work = work;
+  c->chunk = 0;
+  c->grid = xy * c->nbz;
   return OTS_OK;
 }
 
@@ -453,6 +468,7 @@ ots_status validate_tile(ots_plan* pl) {
 void fill_geometry_for_kernel(ots_plan* pl) {
   ots_geometry& g = pl->geo;
   g.kernel = pl->prm.kernel;
+  g.sm_count = pl->sm_count;
   cudaFuncAttributes a{};
   if (g.kernel == OTS_KERNEL_STREAM) {
     const StreamCfg& c = pl->scfg;
@@ -470,14 +486,31 @@ void fill_geometry_for_kernel(ots_plan* pl) {
     g.threads[2] = 1;
     g.e_axis = 1;
     g.shared_bytes = (int64_t)c.smem;
-    g.useful_ratio = (double)c.rpbx * c.rpby * c.zseg / ((double)c.tx * c.ty * (c.zseg + 2 * c.T));
+    {
+      const double n = pl->geo.real_size;
+      g.useful_ratio = (n * n * n) / ((double)c.tx * c.ty * c.nbx * c.nby *
+                                      (double)c.nbz * (c.zseg + 2 * c.T));
+    }
     if (pl->K->stream_attr[c.T][c.eidx] && pl->K->stream_attr[c.T][c.eidx](&a) == cudaSuccess)
       g.registers = a.numRegs;
+    int b = 0;
+    if (pl->K->stream_occ[c.T][c.eidx] &&
+        pl->K->stream_occ[c.T][c.eidx](&b, c.bx * c.by, c.smem) == cudaSuccess)
+      g.ctas_per_sm = b;
   } else if (g.kernel == OTS_KERNEL_PLAIN) {
     if (pl->K->plain_attr(&a) == cudaSuccess) g.registers = a.numRegs;
   } else {
     if (pl->K->tile_attr[g.e_axis][pl->prm.elements_per_thread](&a) == cudaSuccess)
       g.registers = a.numRegs;
+    // resident CTAs per SM from registers, shared memory and threads
+    const int thr = g.threads[0] * g.threads[1] * g.threads[2];
+    if (a.numRegs > 0 && thr > 0) {
+      const int warps = (thr + 31) / 32;
+      const int by_regs = 65536 / (warps * 32 * ((a.numRegs + 7) / 8 * 8));
+      const int by_smem = pl->tile_smem ? (int)(233472 / (pl->tile_smem + 1024)) : 32;
+      const int by_thr = 2048 / thr;
+      g.ctas_per_sm = std::max(0, std::min(std::min(by_regs, by_smem), std::min(by_thr, 32)));
+    }
   }
 }
 
@@ -525,6 +558,10 @@ ots_status enqueue_run(ots_plan* pl, int kernel) {
       sp.out = pl->state[pl->cur ^ 1][0];
       sp.aux = pl->info->na ? pl->aux[0] : nullptr;
       sp.L = pl->L;
+      sp.ntx = c.nbx;
+      sp.nty = c.nby;
+      sp.work = c.work;
+      sp.chunk = c.chunk;
       sp.zseg = c.zseg;
       sp.base_step = base;
       sp.err = pl->d_err;
@@ -537,8 +574,8 @@ ots_status enqueue_run(ots_plan* pl, int kernel) {
         ots_status st = make_tmap(pl, c, pl->state[pl->cur][0], &m);
         if (st != OTS_OK) return st;
       }
-      e = pl->K->stream[Tl][c.eidx](m, sp, dim3(c.nbx, c.nby, c.nbz), dim3(c.bx, c.by, 1), c.smem,
-                                    pl->stream);
+      e = pl->K->stream[Tl][c.eidx](m, sp, dim3(c.nbx * c.nby, c.nbz, 1), dim3(c.bx, c.by, 1),
+                                    c.smem, pl->stream);
       pl->cur ^= 1;
     }
   } else {
@@ -711,39 +748,43 @@ ots_status ots_fill_reference(int32_t dims, int32_t P, int32_t padding, int32_t 
   return OTS_OK;
 }
 
+static ots_status prepare(const ots_params* params, ots_plan* pl);
+
 ots_status ots_derive_geometry(const ots_params* params, ots_geometry* out) {
   if (!out) return fail(OTS_ERR_INVALID_ARGUMENT, "geometry output is NULL");
   const StencilInfo* si = nullptr;
-  return derive(params, out, &si);
+  ots_status st = derive(params, out, &si);
+  if (st != OTS_OK) return st;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return OTS_OK;  // no device: the reference derivation only
+  }
+  // with a device: resolve and validate the kernel as ots_plan_create would
+  ots_plan tmp;
+  st = prepare(params, &tmp);
+  if (st != OTS_OK) return st;
+  *out = tmp.geo;
+  return OTS_OK;
 }
 
-ots_status ots_plan_create(const ots_params* params, ots_plan** out) {
-  if (!out) return fail(OTS_ERR_INVALID_ARGUMENT, "plan output is NULL");
-  *out = nullptr;
-  ots_plan* pl = new ots_plan();
+// Everything plan creation does short of allocating: geometry, operator
+// arguments, kernel resolution and launch validation, device layout.
+static ots_status prepare(const ots_params* params, ots_plan* pl) {
   ots_status st = derive(params, &pl->geo, &pl->info);
-  if (st != OTS_OK) {
-    delete pl;
-    return st;
-  }
+  if (st != OTS_OK) return st;
   pl->prm = *params;
   pl->K = &ots::kernels_for(params->stencil);
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     cudaGetLastError();
-    delete pl;
     return fail(OTS_ERR_NO_DEVICE, "no CUDA device visible");
   }
-  if (params->device < 0 || params->device >= ndev) {
-    delete pl;
+  if (params->device < 0 || params->device >= ndev)
     return fail(OTS_ERR_INVALID_ARGUMENT, "device %d out of range", params->device);
-  }
   pl->device = params->device;
   cudaError_t ce = cudaSetDevice(pl->device);
-  if (ce != cudaSuccess) {
-    delete pl;
-    return cuda_fail(ce, "cudaSetDevice");
-  }
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaSetDevice");
   cudaDeviceProp prop;
   cudaGetDeviceProperties(&prop, pl->device);
   pl->sm_count = prop.multiProcessorCount;
@@ -778,30 +819,39 @@ ots_status ots_plan_create(const ots_params* params, ots_plan** out) {
   // kernel family + launch validation
   int k = 0;
   st = resolve_kernel(pl, OTS_KERNEL_AUTO, &k);
-  if (st != OTS_OK) {
-    delete pl;
-    return st;
-  }
+  if (st != OTS_OK) return st;
   pl->prm.kernel = k;
   if (k == OTS_KERNEL_STREAM) {
     st = derive_stream(pl, p.time_tile, &pl->scfg);
   } else if (k == OTS_KERNEL_TILE) {
     st = validate_tile(pl);
   }
-  if (st != OTS_OK) {
-    delete pl;
-    return st;
-  }
+  if (st != OTS_OK) return st;
 
   // device layout: interior only, rows padded to 32 floats
   const int d = pl->geo.dims, n = pl->geo.real_size;
   pl->L.n0 = n;
   pl->L.n1 = d >= 2 ? n : 1;
   pl->L.n2 = d == 3 ? n : 1;
-  pl->L.sy = d >= 2 ? round_up(n, 32) : round_up(n, 32);
+  pl->L.sy = round_up(n, 32);
   pl->L.sz = pl->L.sy * pl->L.n1;
   pl->field_elems = pl->L.sz * pl->L.n2;
+  fill_geometry_for_kernel(pl);
+  return OTS_OK;
+}
 
+ots_status ots_plan_create(const ots_params* params, ots_plan** out) {
+  if (!out) return fail(OTS_ERR_INVALID_ARGUMENT, "plan output is NULL");
+  if (!params) return fail(OTS_ERR_INVALID_ARGUMENT, "params is NULL");
+  *out = nullptr;
+  ots_plan* pl = new ots_plan();
+  ots_status st = prepare(params, pl);
+  if (st != OTS_OK) {
+    delete pl;
+    return st;
+  }
+  const int k = pl->prm.kernel;
+  cudaError_t ce;
   ce = cudaStreamCreateWithFlags(&pl->stream, cudaStreamNonBlocking);
   if (ce == cudaSuccess) ce = cudaEventCreate(&pl->ev0);
   if (ce == cudaSuccess) ce = cudaEventCreate(&pl->ev1);
@@ -831,7 +881,6 @@ ots_status ots_plan_create(const ots_params* params, ots_plan** out) {
     }
     pl->tmap_ok = true;
   }
-  fill_geometry_for_kernel(pl);
   *out = pl;
   return OTS_OK;
 }

@@ -36,7 +36,10 @@ struct StreamParams {
   float* out;
   const float* aux;  // star stencils use at most one aux field (Poisson f)
   Layout L;
-  int zseg;          // output planes per CTA along z
+  int ntx, nty;      // x/y tiles
+  int64_t work;      // total output tile-planes = ntx * nty * n2
+  int64_t chunk;     // persistent mode: tile-planes per CTA (the last gets fewer)
+  int zseg;          // grid mode (> 0): blockIdx.x = tile, blockIdx.y = z segment
   int base_step;     // global step index of this launch's first level
   int* err;          // device error word (bit 0: mbarrier wait timed out)
   OpArgs op;
@@ -137,6 +140,13 @@ struct Phase {
 // blockDim.x (threads along x) must be 8, 16 or 32: a warp then holds whole
 // rows of the tile, so every x neighbour a shuffle cannot reach (lane 0's
 // left, lane 31's right) is a tile-edge halo cell whose value is never used.
+//
+// Schedules.  Grid mode (zseg > 0): blockIdx.x = x/y tile, blockIdx.y = z
+// segment, so the CTAs resident together stream the same planes of
+// neighbouring tiles and their overlapping halo boxes hit in L2.  Persistent
+// mode (zseg == 0): one CTA per resident slot, each taking an equal
+// contiguous chunk of the (tile, plane) work.  Grid mode is the default: the
+// persistent chunks lose the halo reuse in L2.
 template <class Op, int T, int E>
 __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
     stream_kernel(const __grid_constant__ CUtensorMap tmap,
@@ -149,21 +159,46 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
   const int TX = V * BX, TY = E * BY;
   const int PL = stream_plane_stride(TX, TY);
   const int rpbx = TX - 2 * HX, rpby = TY - 2 * HY;
-  const int tx0 = blockIdx.x * rpbx - HX;  // multiple of 4 (TMA x alignment)
-  const int ty0 = blockIdx.y * rpby - HY;
-  const int zs = blockIdx.z * p.zseg;
-  const int ze = min(zs + p.zseg, p.L.n2);
-  const int kb = zs - T, ke = ze + T - 1, nit = ke - kb + 1;
   const int tid = threadIdx.x + BX * threadIdx.y;
   const int XB = NST * PL;  // exchange planes start (floats)
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + XB + (T > 1 ? (T - 1) * 2 * PL : 0));
   const unsigned box_bytes = (unsigned)(TX * TY) * sizeof(float);
+  const int n2 = p.L.n2;
 
   // per-thread constant shared offsets (floats)
   const int lx = V * threadIdx.x, ly = E * threadIdx.y;
   const int o_top = (ly > 0 ? ly - 1 : 0) * TX + lx;          // clamped: tile-edge halo
   const int o_bot = (ly + E < TY ? ly + E : TY - 1) * TX + lx;
   const int o_row0 = ly * TX + lx;
+  const bool wx = lx >= HX && lx < HX + rpbx;
+
+  if (tid == 0) {
+    for (int s = 0; s < NST; ++s) mbar_init(&bars[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+
+  int64_t pos, pend;
+  if (p.zseg > 0) {  // grid mode: neighbouring tiles stream the same planes together
+    pos = (int64_t)blockIdx.x * n2 + (int64_t)blockIdx.y * p.zseg;
+    pend = (int64_t)blockIdx.x * n2 + min(n2, (int)(blockIdx.y + 1) * p.zseg);
+  } else {
+    pos = (int64_t)blockIdx.x * p.chunk;
+    pend = pos + p.chunk < p.work ? pos + p.chunk : p.work;
+  }
+  int rg = 0;  // running plane counter across segments: ring stage and parity
+  bool ok = true;
+  int fail_r = -1;
+  while (ok && pos < pend) {
+  const int tile = (int)(pos / n2);
+  const int zs = (int)(pos - (int64_t)tile * n2);
+  const int ze = (int)((pend - pos) < (int64_t)(n2 - zs) ? zs + (pend - pos) : n2);
+  pos += ze - zs;
+  const int tyi = tile / p.ntx, txi = tile - tyi * p.ntx;
+  const int tx0 = txi * rpbx - HX;  // multiple of 4 (TMA x alignment)
+  const int ty0 = tyi * rpby - HY;
+  const int kb = zs - T, ke = ze + T - 1, nit = ke - kb + 1;
   const int gx = tx0 + lx, gy = ty0 + ly;
   unsigned xyin = 0;
 #pragma unroll
@@ -173,7 +208,6 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
       if ((unsigned)(gx + v) < (unsigned)p.L.n0 && (unsigned)(gy + e) < (unsigned)p.L.n1)
         xyin |= 1u << (e * V + v);
   const bool xyall = xyin == ((E * V >= 32) ? 0xFFFFFFFFu : ((1u << (E * V)) - 1u));
-  const bool wx = lx >= HX && lx < HX + rpbx;
   float* const obase = p.out + (int64_t)gy * p.L.sy + gx;
   const float* const abase = p.aux + (int64_t)gy * p.L.sy + gx;
 
@@ -188,32 +222,29 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
 #pragma unroll
         for (int v = 0; v < V; ++v) R[t][s][e][v] = 0.0f;
 
-  if (tid == 0) {
-    for (int s = 0; s < NST; ++s) mbar_init(&bars[s], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  }
+  // every thread is past the previous segment's reads of the ring
   __syncthreads();
   if (tid == 0) {
     for (int j = 0; j < LA && j < nit; ++j) {
-      mbar_arrive_expect_tx(&bars[j], box_bytes);
-      tma_load_3d(smem + j * PL, &tmap, tx0, ty0, kb + j, &bars[j]);
+      const int g = rg + j;
+      mbar_arrive_expect_tx(&bars[g & (NST - 1)], box_bytes);
+      tma_load_3d(smem + (g & (NST - 1)) * PL, &tmap, tx0, ty0, kb + j, &bars[g & (NST - 1)]);
     }
   }
 
-  int fail_r = -1;
   auto step = [&](auto ph, int r) -> bool {
     constexpr int PH = decltype(ph)::value;
     constexpr int SN = PH, SC = (PH + 2) % 3, SM = (PH + 1) % 3;  // newest, centre, z-1
     const int k = kb + r;
-    const int st = r & (NST - 1);
-    const bool to = !mbar_wait_bounded(&bars[st], (r / NST) & 1, p.err);
+    const int g = rg + r;  // running plane index: ring stage and phase parity
+    const int st = g & (NST - 1);
+    const bool to = !mbar_wait_bounded(&bars[st], (g / NST) & 1, p.err);
     if (__syncthreads_or(to)) {
-      fail_r = r;
+      fail_r = g;
       return false;
     }
     if (tid == 0 && r + LA < nit) {
-      const int s2 = (r + LA) & (NST - 1);
+      const int s2 = (g + LA) & (NST - 1);
       mbar_arrive_expect_tx(&bars[s2], box_bytes);
       tma_load_3d(smem + s2 * PL, &tmap, tx0, ty0, k + LA, &bars[s2]);
     }
@@ -224,7 +255,7 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
       const float4 a = *reinterpret_cast<const float4*>(smem + pk + o_row0 + e * TX);
       R[0][SN][e][0] = a.x; R[0][SN][e][1] = a.y; R[0][SN][e][2] = a.z; R[0][SN][e][3] = a.w;
     }
-    const int pc0 = ((r + NST - 1) & (NST - 1)) * PL;   // input plane k-1 (level 1 centre)
+    const int pc0 = ((g + NST - 1) & (NST - 1)) * PL;   // input plane k-1 (level 1 centre)
     const int xr = XB + ((r - 1) & 1) * PL;              // exchange planes of iteration r-1
     const int xw = XB + (r & 1) * PL;                    // exchange planes of iteration r
 #pragma unroll
@@ -257,7 +288,9 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
       }
       const float tvv[V] = {tv.x, tv.y, tv.z, tv.w};
       const float bvv[V] = {bv.x, bv.y, bv.z, bv.w};
-      float out[E][V];
+      // level T writes the ring slot of level T-1's oldest plane, which no
+      // level needs any more (a scratch slot); levels < T write their own ring
+      float (&out)[E][V] = (t < T) ? R[t < T ? t : 0][SN] : R[T - 1][SM];
 #pragma unroll
       for (int e = 0; e < E; ++e)
 #pragma unroll
@@ -285,10 +318,6 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
         if (E > 1)
           *reinterpret_cast<float4*>(smem + xb + o_row0 + (E - 1) * TX) =
               make_float4(out[E - 1][0], out[E - 1][1], out[E - 1][2], out[E - 1][3]);
-#pragma unroll
-        for (int e = 0; e < E; ++e)
-#pragma unroll
-          for (int v = 0; v < V; ++v) R[t][SN][e][v] = out[e][v];
       } else if (q >= zs && q < ze && wx) {
         float* dst = obase + (int64_t)q * p.L.sz;
 #pragma unroll
@@ -310,7 +339,6 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
     return true;
   };
 
-  bool ok = true;
   int r = 0;
   for (; r + 2 < nit && ok; r += 3) {
     ok = step(Phase<0>{}, r);
@@ -319,16 +347,18 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
   }
   if (ok && r < nit) ok = step(Phase<0>{}, r++);
   if (ok && r < nit) ok = step(Phase<1>{}, r++);
+  if (ok) rg += nit;
   if (!ok) {
     if (tid == 0) {
       atomicOr(p.err, 1);
       // drain this CTA's copies still in flight (bounded) before leaving:
-      // planes fail_r .. fail_r + LA - 1 were issued
-      for (int j = fail_r; j < nit && j < fail_r + LA; ++j)
+      // running planes fail_r .. fail_r + LA - 1 were issued
+      for (int j = fail_r; j < rg + nit && j < fail_r + LA; ++j)
         mbar_wait_bounded(&bars[j & (NST - 1)], (j / NST) & 1, p.err);
     }
     __syncthreads();
   }
+  }  // segments
 }
 
 }  // namespace ots

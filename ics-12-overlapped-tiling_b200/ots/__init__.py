@@ -71,7 +71,8 @@ class Geometry(ctypes.Structure):
                 ("registers", ctypes.c_int32), ("shared_bytes", ctypes.c_int64),
                 ("interior_points", ctypes.c_int64), ("flops_per_point", ctypes.c_double),
                 ("useful_ratio", ctypes.c_double), ("coef", ctypes.c_float),
-                ("h2", ctypes.c_float)]
+                ("h2", ctypes.c_float), ("ctas_per_sm", ctypes.c_int32),
+                ("sm_count", ctypes.c_int32)]
 
     def as_dict(self):
         out = {}

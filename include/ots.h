@@ -144,6 +144,8 @@ typedef struct ots_geometry {
   double useful_ratio;         /* reference "Useful Ratio" */
   float coef;                  /* averaging weight in effect */
   float h2;                    /* Poisson h^2 in effect */
+  int32_t ctas_per_sm;         /* resident CTAs per SM of the chosen kernel */
+  int32_t sm_count;            /* SMs of the device */
 } ots_geometry;
 
 typedef struct ots_timing {
@@ -190,7 +192,9 @@ void ots_plan_destroy(ots_plan* plan);
 ots_status ots_plan_geometry(const ots_plan* plan, ots_geometry* out);
 
 /* Derive the geometry without allocating (what the reference prints before
- * running).  Same validation as ots_plan_create. */
+ * running).  With a CUDA device visible this also resolves and validates the
+ * kernel exactly as ots_plan_create does (registers, shared bytes, resident
+ * CTAs per SM); without one it is the reference derivation only. */
 ots_status ots_derive_geometry(const ots_params* params, ots_geometry* out);
 
 /* Copy host fields (reference layout, P^d each) into the plan.  `state` has
@@ -233,6 +237,37 @@ ots_status ots_plan_stream(const ots_plan* plan, void** cuda_stream);
 /* Page-lock a caller's host buffer so uploads/downloads run as async DMA. */
 ots_status ots_host_register(void* ptr, size_t bytes);
 ots_status ots_host_unregister(void* ptr);
+
+/* ---- learned cost model --------------------------------------------------
+ * A multi-layer perceptron (n_in -> hidden x (layers-1), SiLU -> 1) trained
+ * and evaluated on the GPU by the library's own kernels.  It replaces the
+ * reference's Weka k-NN cost model (scripts/run-weka.py:49-150, features from
+ * scripts/extract-features.py:40-127): trained on measured sweeps, it ranks a
+ * configuration space so that only the top k need measuring. */
+typedef struct ots_mlp ots_mlp;
+
+ots_status ots_mlp_create(int32_t n_in, int32_t hidden, int32_t layers, uint64_t seed,
+                          int32_t device, ots_mlp** out);
+void ots_mlp_destroy(ots_mlp* model);
+ots_status ots_mlp_num_params(const ots_mlp* model, int64_t* n);
+/* Parameters, layer by layer: W (out x in, row-major) then b (out). */
+ots_status ots_mlp_get_params(const ots_mlp* model, float* params);
+ots_status ots_mlp_set_params(ots_mlp* model, const float* params);
+/* Inputs are standardised as (x - mean) * inv_std; targets as (y - y_mean) / y_std. */
+ots_status ots_mlp_set_normalization(ots_mlp* model, const float* mean, const float* inv_std,
+                                     float y_mean, float y_std);
+/* Mean squared error on the standardised targets of n rows (n <= 4096) and
+ * its gradient with respect to every parameter (grad may be NULL). */
+ots_status ots_mlp_loss_grad(ots_mlp* model, const float* X, const float* y, int32_t n,
+                             float* loss, float* grad);
+/* AdamW minibatch training; each epoch is one replay of a captured CUDA
+ * graph.  final_loss = mean minibatch loss of the last epoch. */
+ots_status ots_mlp_train(ots_mlp* model, const float* X, const float* y, int32_t n,
+                         int32_t epochs, int32_t batch, float lr, float weight_decay,
+                         uint64_t seed, float* final_loss);
+ots_status ots_mlp_predict(ots_mlp* model, const float* X, int32_t n, float* y_out);
+/* Indices of the k largest predictions, best first. */
+ots_status ots_mlp_topk(ots_mlp* model, const float* X, int32_t n, int32_t k, int32_t* idx_out);
 
 #ifdef __cplusplus
 }

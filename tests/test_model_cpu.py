@@ -1,0 +1,54 @@
+"""CPU checks of the picker's pieces: the MLP oracle's backprop against
+finite differences, the feature builder, and the random-k baseline."""
+import math
+
+import numpy as np
+
+import mlp_ref
+from ots import model
+
+
+def test_mlp_oracle_backprop_matches_finite_differences():
+    rng = np.random.default_rng(0)
+    dims = mlp_ref.layer_dims(5, 7, 3)
+    n_par = sum(i * o + o for i, o in zip(dims[:-1], dims[1:]))
+    p = rng.normal(0, 0.5, n_par)
+    X = rng.normal(0, 1, (20, 5))
+    y = rng.normal(0, 1, 20)
+    mean, inv = X.mean(0), 1.0 / X.std(0)
+    loss, g = mlp_ref.loss_grad(X, y, p, dims, mean, inv, 0.1, 1.3)
+    eps = 1e-6
+    for j in rng.choice(n_par, 25, replace=False):
+        q = p.copy()
+        q[j] += eps
+        lp, _ = mlp_ref.loss_grad(X, y, q, dims, mean, inv, 0.1, 1.3)
+        q[j] -= 2 * eps
+        lm, _ = mlp_ref.loss_grad(X, y, q, dims, mean, inv, 0.1, 1.3)
+        assert abs((lp - lm) / (2 * eps) - g[j]) < 1e-6 * max(1.0, abs(g[j]))
+
+
+def _geom(**kw):
+    g = dict(dims=3, radius=1, threads=[16, 16, 1], num_blocks=[10, 20, 7], ctas_per_sm=2,
+             sm_count=148, useful_ratio=0.6, shared_bytes=65664, registers=125,
+             interior_points=512 ** 3, comps=[64, 32, 80])
+    g.update(kw)
+    return g
+
+
+def test_features_are_finite_and_named():
+    cfg = dict(kernel="stream", T=3, bx=16, by=16, bz=1, E=2)
+    f = model.features("jacobi-3d", cfg, _geom())
+    assert f.shape == (len(model.FEATURES),) and np.isfinite(f).all()
+    f2 = model.features("jacobi-3d", dict(cfg, T=1), _geom())
+    i = model.FEATURES.index("bytes_per_update")
+    assert f2[i] == 3 * f[i]
+    assert f[model.FEATURES.index("is_stream")] == 1.0
+
+
+def test_expected_best_of_random_matches_monte_carlo():
+    rng = np.random.default_rng(1)
+    v = rng.random(40)
+    exact = model.expected_best_of_random(v, 4)
+    mc = np.mean([np.max(rng.choice(v, 4, replace=False)) for _ in range(40000)])
+    assert abs(exact - mc) < 5e-3
+    assert model.expected_best_of_random(v, 40) == max(v)
