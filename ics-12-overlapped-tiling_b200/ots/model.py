@@ -248,7 +248,7 @@ def leave_one_out(records, k_frac=0.10, hidden=64, layers=3, epochs=300, batch=1
         loss = m.fit(X[tr], y[tr], epochs=epochs, batch=batch, lr=lr, weight_decay=weight_decay,
                      seed=seed)
         actual = np.exp(y[te].astype(np.float64))
-        k = max(1, int(math.ceil(k_frac * len(te))))
+        k = max(1, int(math.floor(k_frac * len(te))))
         top = m.topk(X[te], k)
         picked = float(np.max(actual[top]))
         top1 = float(actual[top[0]])

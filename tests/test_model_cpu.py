@@ -52,3 +52,18 @@ def test_expected_best_of_random_matches_monte_carlo():
     mc = np.mean([np.max(rng.choice(v, 4, replace=False)) for _ in range(40000)])
     assert abs(exact - mc) < 5e-3
     assert model.expected_best_of_random(v, 40) == max(v)
+
+
+def test_committed_b200_picker_report():
+    """The committed leave-one-stencil-out report measured on B200."""
+    import json
+    import os
+    rep = json.load(open(os.path.join(os.path.dirname(model.__file__), "data",
+                                      "picker_report_b200.json")))
+    stencils = [s for s in rep if not s.startswith("_")]
+    assert len(stencils) == 13
+    for s in stencils:
+        assert rep[s]["picked_over_best"] >= 0.95, s
+    m = rep["_mean"]
+    assert m["picked_over_best"] > m["random_k_over_best"]
+    assert m["top1_over_best"] > m["random_k_over_best"]

@@ -55,3 +55,21 @@ def test_topk_orders_predictions():
     p = m.predict(X)
     top = m.topk(X, 5)
     assert list(top) == list(np.argsort(-p, kind="stable")[:5])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("held", ["rician-denoise-2d", "cdsc-tv-update-2d"])
+def test_learned_picker_finds_near_best_at_tenth_of_the_sweep(held):
+    """Held-out stencils (trained on every other stencil's B200 sweep): the
+    model's top 10 % contains a configuration within 5 % of the exhaustive
+    best, and does at least as well as 10 % random picks (the method without
+    the model at the same measuring cost)."""
+    import json
+    import os
+    data = os.path.join(os.path.dirname(model.__file__), "data", "sweeps_b200.json")
+    recs = json.load(open(data))["records"]
+    rep = model.leave_one_out(recs, held_out=[held], epochs=300)
+    r = rep[held]
+    assert r["measure_cost"] <= 0.10
+    assert r["picked_over_best"] >= 0.95
+    assert r["picked_over_best"] >= r["random_k_over_best"]
