@@ -94,12 +94,24 @@ struct TileThreads {
   static constexpr int kMax = (E * NS <= 2) ? 1024 : (E * NS <= 4) ? 512 : 256;
 };
 
-template <class Op, int E, int EAX>
-__global__ void __launch_bounds__(TileThreads<E, Op::NS>::kMax) tile_kernel(const StepParams p) {
+// Loads for the tile: through the read-only path in the plain tile kernel;
+// at L2 (ld.global.cg) in the batched kernel, whose inputs other CTAs of the
+// same launch have just written.
+template <bool CG>
+__device__ __forceinline__ float tile_load(const float* p) {
+  if constexpr (CG)
+    return __ldcg(p);
+  else
+    return __ldg(p);
+}
+
+// One CTA's overlapped time tile.  (bix, biy, biz) is the tile index, (BX,
+// BY, BZ) the logical thread block and (tx, ty, tz) this thread in it.
+template <class Op, int E, int EAX, bool CG>
+__device__ __forceinline__ void tile_body(const StepParams& p, int bix, int biy, int biz, int bx,
+                                          int by, int bz, int tx, int ty, int tz, float* smem) {
   constexpr int NS = Op::NS, NA = Op::NA;
   constexpr int RX = Op::RX, RY = Op::RY, RZ = Op::RZ;
-  extern __shared__ float smem[];
-  const int bx = blockDim.x, by = blockDim.y, bz = blockDim.z;
   const int cx = bx * (EAX == 0 ? E : 1);
   const int cy = by * (EAX == 1 ? E : 1);
   const int cz = bz * (EAX == 2 ? E : 1);
@@ -107,10 +119,10 @@ __global__ void __launch_bounds__(TileThreads<E, Op::NS>::kMax) tile_kernel(cons
   const int LxLy = Lx * Ly, Lvol = LxLy * Lz;
   const int T = p.T;
   // global coordinate of comps cell 0
-  const int ox = blockIdx.x * p.rpb[0] - RX * (T - 1);
-  const int oy = blockIdx.y * p.rpb[1] - RY * (T - 1);
-  const int oz = blockIdx.z * p.rpb[2] - RZ * (T - 1);
-  const int tid = threadIdx.x + bx * (threadIdx.y + by * threadIdx.z);
+  const int ox = bix * p.rpb[0] - RX * (T - 1);
+  const int oy = biy * p.rpb[1] - RY * (T - 1);
+  const int oz = biz * p.rpb[2] - RZ * (T - 1);
+  const int tid = tx + bx * (ty + by * tz);
   const int nth = bx * by * bz;
   if (p.phase_limit == 1) return;
 
@@ -127,7 +139,7 @@ __global__ void __launch_bounds__(TileThreads<E, Op::NS>::kMax) tile_kernel(cons
       const int64_t gi = (int64_t)gz * p.L.sz + (int64_t)gy * p.L.sy + gx;
 #pragma unroll
       for (int f = 0; f < NS; ++f) {
-        const float v = in ? __ldg(p.in[f] + gi) : 0.0f;
+        const float v = in ? tile_load<CG>(p.in[f] + gi) : 0.0f;
         cur[f * Lvol + i] = v;
         nxt[f * Lvol + i] = v;  // the ring of the second buffer stays defined
       }
@@ -140,10 +152,10 @@ __global__ void __launch_bounds__(TileThreads<E, Op::NS>::kMax) tile_kernel(cons
   float auxv[E][NA > 0 ? NA : 1];
 #pragma unroll
   for (int e = 0; e < E; ++e) {
-    int lx = threadIdx.x, ly = threadIdx.y, lz = threadIdx.z;
-    if (EAX == 0) lx = threadIdx.x + e * bx;
-    if (EAX == 1) ly = threadIdx.y * E + e;
-    if (EAX == 2) lz = threadIdx.z * E + e;
+    int lx = tx, ly = ty, lz = tz;
+    if (EAX == 0) lx = tx + e * bx;
+    if (EAX == 1) ly = ty * E + e;
+    if (EAX == 2) lz = tz * E + e;
     sidx[e] = (lz + RZ) * LxLy + (ly + RY) * Lx + (lx + RX);
     gxs[e] = ox + lx;
     gys[e] = oy + ly;
@@ -151,7 +163,7 @@ __global__ void __launch_bounds__(TileThreads<E, Op::NS>::kMax) tile_kernel(cons
     ins[e] = in_domain(p.L, gxs[e], gys[e], gzs[e]);
     const int64_t gi = (int64_t)gzs[e] * p.L.sz + (int64_t)gys[e] * p.L.sy + gxs[e];
 #pragma unroll
-    for (int a = 0; a < NA; ++a) auxv[e][a] = ins[e] ? __ldg(p.aux[a] + gi) : 0.0f;
+    for (int a = 0; a < NA; ++a) auxv[e][a] = ins[e] ? tile_load<CG>(p.aux[a] + gi) : 0.0f;
   }
   __syncthreads();
 
@@ -192,6 +204,13 @@ __global__ void __launch_bounds__(TileThreads<E, Op::NS>::kMax) tile_kernel(cons
       for (int f = 0; f < NS; ++f) p.out[f][gi] = cur[f * Lvol + sidx[e]];
     }
   }
+}
+
+template <class Op, int E, int EAX>
+__global__ void __launch_bounds__(TileThreads<E, Op::NS>::kMax) tile_kernel(const StepParams p) {
+  extern __shared__ float smem[];
+  tile_body<Op, E, EAX, false>(p, blockIdx.x, blockIdx.y, blockIdx.z, blockDim.x, blockDim.y,
+                               blockDim.z, threadIdx.x, threadIdx.y, threadIdx.z, smem);
 }
 
 // ------------------------------------------------------------------------

@@ -1,0 +1,213 @@
+"""Batched grids: many uneven 2D grids in one persistent, graph-captured launch.
+
+    python -m ots.batch [--grids 256] [--seed 2012] [--reps 5]
+
+runs the batched workload -- 256 independent FP32 grids mixing jacobi-2d,
+poisson-2d (Jacobi sweep with RHS) and gradient-2d, sides log-uniform in
+[64, 2048], step counts uniform in 8..256, inputs uniform [0, 1) -- with each
+grid's (T, block, E) picked by the learned cost model, and prints one JSON
+line: aggregate GUpdates/s of the single graph launch against the same grids
+run one after another (one launch per step, and one tile launch per T steps).
+"""
+import argparse
+import ctypes
+import json
+import math
+import os
+
+import numpy as np
+
+from . import (KERNEL_PLAIN, KERNEL_TILE, OtsError, Params, SID, Timing, check, derive_geometry,
+               lib, make_params)
+
+BATCH_STENCILS = ("jacobi-2d", "poisson-2d", "gradient-2d")
+MENU = [dict(T=T, bx=bx, E=E) for T in range(1, 9) for bx in (16, 32, 64) for E in (1, 2, 4)]
+
+
+def _blib():
+    L = lib()
+    if not getattr(L, "_batch_ready", False):
+        vp = ctypes.c_void_p
+        L.ots_batch_create.argtypes = [ctypes.POINTER(Params), ctypes.c_int32, ctypes.c_int32,
+                                       ctypes.POINTER(vp)]
+        L.ots_batch_create.restype = ctypes.c_int
+        L.ots_batch_destroy.argtypes = [vp]
+        L.ots_batch_destroy.restype = None
+        L.ots_batch_info.argtypes = [vp, ctypes.POINTER(ctypes.c_int64),
+                                     ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
+        L.ots_batch_info.restype = ctypes.c_int
+        F = ctypes.POINTER(ctypes.c_float)
+        L.ots_batch_upload.argtypes = [vp, ctypes.c_int32, F, F]
+        L.ots_batch_upload.restype = ctypes.c_int
+        L.ots_batch_download.argtypes = [vp, ctypes.c_int32, F]
+        L.ots_batch_download.restype = ctypes.c_int
+        L.ots_batch_run.argtypes = [vp, ctypes.POINTER(Timing)]
+        L.ots_batch_run.restype = ctypes.c_int
+        L.ots_batch_run_async.argtypes = [vp]
+        L.ots_batch_run_async.restype = ctypes.c_int
+        L.ots_batch_stream.argtypes = [vp, ctypes.POINTER(vp)]
+        L.ots_batch_stream.restype = ctypes.c_int
+        L.ots_batch_run_sequential.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(Timing)]
+        L.ots_batch_run_sequential.restype = ctypes.c_int
+        L._batch_ready = True
+    return L
+
+
+def workload(count=256, seed=2012):
+    """The batched benchmark's grids (seeded): stencil uniform over the three,
+    side round(exp(U[ln 64, ln 2048])), steps uniform 8..256."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        st = BATCH_STENCILS[int(rng.integers(0, 3))]
+        n = int(round(math.exp(rng.uniform(math.log(64), math.log(2048)))))
+        steps = int(rng.integers(8, 257))
+        out.append(dict(stencil=st, n=n, steps=steps))
+    return out
+
+
+def pick(grids, cost_model=None, device=0):
+    """Choose (T, bx, E) per grid from MENU: the cost model's best predicted
+    configuration, or T=4, 32 x 8, E=2 without a model."""
+    from . import model as M
+    for g in grids:
+        if cost_model is None:
+            g.update(T=4, bx=32, E=2)
+            continue
+        feats, cands = [], []
+        for c in MENU:
+            cfg = dict(kernel="tile", T=c["T"], bx=c["bx"], by=256 // c["bx"], bz=1, E=c["E"])
+            try:
+                geo = derive_geometry(stencil=g["stencil"], n=g["n"], steps=g["steps"], T=c["T"],
+                                      bx=c["bx"], by=256 // c["bx"], bz=1, E=c["E"],
+                                      kernel="tile", device=device)
+            except OtsError:
+                continue
+            feats.append(M.features(g["stencil"], cfg, geo))
+            cands.append(c)
+        best = int(cost_model.topk(np.stack(feats), 1)[0])
+        g.update(cands[best])
+    return grids
+
+
+class Batch:
+    def __init__(self, grids, device=0):
+        arr = (Params * len(grids))()
+        for i, g in enumerate(grids):
+            arr[i] = make_params(g["stencil"], g["n"], g["steps"], T=g["T"], bx=g["bx"],
+                                 by=256 // g["bx"], E=g["E"], device=device)
+        h = ctypes.c_void_p()
+        check(_blib().ots_batch_create(arr, len(grids), device, ctypes.byref(h)))
+        self.h = h
+        self.grids = grids
+
+    def close(self):
+        if getattr(self, "h", None):
+            _blib().ots_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self):
+        u, it, c = ctypes.c_int64(), ctypes.c_int32(), ctypes.c_int32()
+        check(_blib().ots_batch_info(self.h, ctypes.byref(u), ctypes.byref(it), ctypes.byref(c)))
+        return {"updates": u.value, "items": it.value, "ctas": c.value}
+
+    def upload(self, i, state, aux=None):
+        F = ctypes.POINTER(ctypes.c_float)
+        s = np.ascontiguousarray(state, np.float32)
+        n = self.grids[i]["n"]
+        assert s.shape == (n, n)
+        a = None if aux is None else np.ascontiguousarray(aux, np.float32)
+        check(_blib().ots_batch_upload(self.h, i, s.ctypes.data_as(F),
+                                       None if a is None else a.ctypes.data_as(F)))
+
+    def download(self, i):
+        n = self.grids[i]["n"]
+        out = np.zeros((n, n), np.float32)
+        check(_blib().ots_batch_download(self.h, i, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return out
+
+    def run(self):
+        t = Timing()
+        check(_blib().ots_batch_run(self.h, ctypes.byref(t)))
+        return t.event_ms * 1e-3
+
+    def run_sequential(self, kernel="plain"):
+        t = Timing()
+        k = KERNEL_PLAIN if kernel == "plain" else KERNEL_TILE
+        check(_blib().ots_batch_run_sequential(self.h, k, ctypes.byref(t)))
+        return t.event_ms * 1e-3, t.launches
+
+
+def inputs(grids, seed=7):
+    """Uniform [0, 1) interiors (and f in [-1, 1) for Poisson), seeded."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for g in grids:
+        s = rng.random((g["n"], g["n"]), dtype=np.float32)
+        a = (2.0 * rng.random((g["n"], g["n"]), dtype=np.float32) - 1.0) \
+            if g["stencil"] == "poisson-2d" else None
+        out.append((s, a))
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--grids", type=int, default=256)
+    ap.add_argument("--seed", type=int, default=2012)
+    ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--no-model", action="store_true")
+    a = ap.parse_args(argv)
+    from . import model as M
+    cm = None
+    if not a.no_model:
+        path = os.path.join(os.path.dirname(__file__), "data", "cost_model.json")
+        cm = M.MLP.from_json(json.load(open(path)))
+    grids = pick(workload(a.grids, a.seed), cm)
+    b = Batch(grids)
+    ins = inputs(grids)
+
+    def load():
+        for i, (s, x) in enumerate(ins):
+            b.upload(i, s, x)
+
+    load()
+    b.run()  # warm-up
+    t_graph = []
+    for _ in range(a.reps):
+        load()
+        t_graph.append(b.run())
+    load()
+    b.run_sequential("tile")
+    t_tile = []
+    for _ in range(max(1, a.reps // 2)):
+        load()
+        t_tile.append(b.run_sequential("tile")[0])
+    load()
+    t_plain, launches = b.run_sequential("plain")
+    info = b.info()
+    upd = info["updates"]
+    tg = sorted(t_graph)[len(t_graph) // 2]
+    tt = sorted(t_tile)[len(t_tile) // 2]
+    print(json.dumps({
+        "metric": "GUpdates/s", "workload": "batched: %d grids jacobi-2d/poisson-2d/gradient-2d, "
+        "sides 64..2048 log-uniform, steps 8..256 (seed %d)" % (a.grids, a.seed),
+        "updates": upd, "items": info["items"], "ctas": info["ctas"],
+        "graph_one_launch": {"value": upd / tg / 1e9, "seconds": tg},
+        "sequential_tile": {"value": upd / tt / 1e9, "seconds": tt},
+        "sequential_plain": {"value": upd / t_plain / 1e9, "seconds": t_plain,
+                             "launches": launches},
+        "speedup_vs_sequential_plain": t_plain / tg, "speedup_vs_sequential_tile": tt / tg,
+        "configs_from": "cost model" if cm is not None else "default T=4 32x8 E=2",
+    }))
+    b.close()
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -238,6 +238,33 @@ ots_status ots_plan_stream(const ots_plan* plan, void** cuda_stream);
 ots_status ots_host_register(void* ptr, size_t bytes);
 ots_status ots_host_unregister(void* ptr);
 
+/* ---- batched grids ---------------------------------------------------------
+ * Many independent 2D grids (jacobi-2d, poisson-2d Jacobi sweep with RHS,
+ * gradient-2d) of uneven sizes and step counts, each with its own
+ * (T, block_x in {16, 32, 64} x 256/block_x threads, E in {1, 2, 4}), run as
+ * ONE persistent kernel launch captured in a CUDA graph.  No reference
+ * counterpart: the reference runs one grid per process
+ * (opencl/jacobi-2d/jacobi-2d.cpp:553-1048).  `grids` uses ots_params; the
+ * fields read are stencil, problem_size, time_steps, time_tile, block_x,
+ * elements_per_thread, coef and h2 (Poisson uses the BASELINE variant). */
+typedef struct ots_batch ots_batch;
+
+ots_status ots_batch_create(const ots_params* grids, int32_t n, int32_t device, ots_batch** out);
+void ots_batch_destroy(ots_batch* batch);
+/* Total grid-point updates of one run, queue items, persistent CTAs. */
+ots_status ots_batch_info(const ots_batch* batch, int64_t* updates, int32_t* items,
+                          int32_t* ctas);
+/* Dense n x n interior arrays (x fastest); aux is Poisson's f (else NULL). */
+ots_status ots_batch_upload(ots_batch* batch, int32_t grid, const float* state, const float* aux);
+ots_status ots_batch_download(ots_batch* batch, int32_t grid, float* state);
+/* One graph launch running every grid to its step count. */
+ots_status ots_batch_run(ots_batch* batch, ots_timing* timing);
+ots_status ots_batch_run_async(ots_batch* batch);
+ots_status ots_batch_stream(const ots_batch* batch, void** cuda_stream);
+/* Comparator on the same buffers: the grids one after another with one
+ * launch per step (OTS_KERNEL_PLAIN) or per T steps (OTS_KERNEL_TILE). */
+ots_status ots_batch_run_sequential(ots_batch* batch, int32_t kernel, ots_timing* timing);
+
 /* ---- learned cost model --------------------------------------------------
  * A multi-layer perceptron (n_in -> hidden x (layers-1), SiLU -> 1) trained
  * and evaluated on the GPU by the library's own kernels.  It replaces the
