@@ -12,7 +12,7 @@ GRIDS = [
     dict(stencil="poisson-2d", n=67, steps=9, T=3, bx=16, E=4),
     dict(stencil="gradient-2d", n=45, steps=7, T=2, bx=64, E=1),
     dict(stencil="jacobi-2d", n=17, steps=30, T=8, bx=64, E=4),
-    dict(stencil="poisson-2d", n=100, steps=1, T=5, bx=32, E=1),
+    dict(stencil="poisson-2d", n=100, steps=1, T=5, bx=32, E=2),
     dict(stencil="jacobi-2d", n=64, steps=0, T=2, bx=16, E=2),
     dict(stencil="gradient-2d", n=90, steps=12, T=4, bx=32, E=4),
     dict(stencil="jacobi-2d", n=200, steps=16, T=1, bx=16, E=1),
@@ -79,7 +79,7 @@ def test_batch_rejects_unsupported_grids():
         B.Batch([dict(stencil="jacobi-2d", n=32, steps=4, T=2, bx=8, E=2)])
     assert ei.value.status_name == "UNSUPPORTED"
     with pytest.raises(OtsError) as ei:
-        B.Batch([dict(stencil="jacobi-2d", n=32, steps=4, T=8, bx=16, E=1)])
+        B.Batch([dict(stencil="jacobi-2d", n=32, steps=4, T=4, bx=64, E=1)])
     assert ei.value.status_name == "INVALID_GEOMETRY"
 
 
