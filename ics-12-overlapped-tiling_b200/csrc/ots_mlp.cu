@@ -16,6 +16,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -176,6 +177,26 @@ __global__ void k_adamw(float* __restrict__ w, const float* __restrict__ g, floa
 }
 
 inline int cdiv(int a, int b) { return (a + b - 1) / b; }
+
+// y = z * scale + shift (undo the target standardisation)
+__global__ void k_affine(const float* __restrict__ z, float* __restrict__ y, int n, float scale,
+                         float shift) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = z[i] * scale + shift;
+}
+
+// Fixed-size working memory of ots_mlp_predict_noalloc: two ping-pong
+// activation buffers of kNoAllocRows x kNoAllocWidth floats (2 MiB in all).
+// It lives in the module image, so every GPU that loads libots holds it until
+// the process exits; no call allocates it.
+constexpr int kNoAllocRows = 4096;
+constexpr int kNoAllocWidth = 64;
+__device__ __align__(256) float g_noalloc_scratch[2 * kNoAllocRows * kNoAllocWidth];
+
+// Device address of g_noalloc_scratch, looked up once per device.
+constexpr int kMaxDevices = 64;
+float* g_noalloc_ptr[kMaxDevices] = {};
+std::mutex g_noalloc_mu;
 
 }  // namespace
 
@@ -544,6 +565,62 @@ ots_status ots_mlp_predict(ots_mlp* m, const float* X, int32_t n, float* y_out) 
   cudaFree(dX);
   if (e != cudaSuccess) return mfail(OTS_ERR_CUDA, "predict: %s", cudaGetErrorString(e));
   for (int i = 0; i < n; ++i) y_out[i] = yn[i] * m->y_std + m->y_mean;
+  return OTS_OK;
+}
+
+// Inference with no allocation (see include/ots.h).  X and y are device
+// pointers; the activations live in g_noalloc_scratch, whose device address
+// is looked up with cudaGetSymbolAddress on the first call on each device.
+ots_status ots_mlp_predict_noalloc(const ots_mlp* m, const float* X, int32_t n, float* y,
+                                   void* stream) {
+  if (!m || !X || !y) return mfail(OTS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (n < 1 || n > kNoAllocRows)
+    return mfail(OTS_ERR_INVALID_ARGUMENT,
+                 "ots_mlp_predict_noalloc: n = %d rows; the fixed scratch holds 1..%d rows", n,
+                 kNoAllocRows);
+  for (int l = 0; l <= m->layers; ++l)
+    if (m->dims[l] > kNoAllocWidth)
+      return mfail(OTS_ERR_UNSUPPORTED,
+                   "ots_mlp_predict_noalloc: layer width %d exceeds the fixed scratch width %d",
+                   m->dims[l], kNoAllocWidth);
+  int dev = -1;
+  MLP_CUDA(cudaGetDevice(&dev));
+  if (dev != m->device)
+    return mfail(OTS_ERR_INVALID_ARGUMENT,
+                 "ots_mlp_predict_noalloc: current device %d is not the model's device %d", dev,
+                 m->device);
+  if (dev < 0 || dev >= kMaxDevices)
+    return mfail(OTS_ERR_UNSUPPORTED, "ots_mlp_predict_noalloc: device %d out of range", dev);
+  float* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+      void* p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess)
+        return mfail(OTS_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch): %s",
+                     cudaGetErrorString(e));
+      g_noalloc_ptr[dev] = static_cast<float*>(p);
+    }
+    scratch = g_noalloc_ptr[dev];
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  float* buf[2] = {scratch, scratch + (size_t)kNoAllocRows * kNoAllocWidth};
+  // every element read below is written first in this call, so the previous
+  // call's contents never leak into the result
+  k_normalize<<<cdiv(n * m->n_in, 256), 256, 0, s>>>(X, m->d_mean, m->d_inv_std, buf[0], n,
+                                                     m->n_in);
+  int cur = 0;
+  for (int l = 0; l < m->layers; ++l) {
+    const int I = m->dims[l], O = m->dims[l + 1];
+    gemm(s, n, O, I, buf[cur], I, 0, m->d_params + m->w_off[l], I, 1, buf[cur ^ 1], O,
+         m->d_params + m->b_off[l]);
+    if (l < m->layers - 1)
+      k_silu<<<cdiv(n * O, 256), 256, 0, s>>>(buf[cur ^ 1], buf[cur ^ 1], n * O);
+    cur ^= 1;
+  }
+  k_affine<<<cdiv(n, 256), 256, 0, s>>>(buf[cur], y, n, m->y_std, m->y_mean);
+  MLP_CUDA(cudaGetLastError());
   return OTS_OK;
 }
 

@@ -296,6 +296,27 @@ ots_status ots_mlp_predict(ots_mlp* model, const float* X, int32_t n, float* y_o
 /* Indices of the k largest predictions, best first. */
 ots_status ots_mlp_topk(ots_mlp* model, const float* X, int32_t n, int32_t k, int32_t* idx_out);
 
+/* Cost-model inference that allocates nothing -- no counterpart in the
+ * reference.  For callers that must not call cudaMalloc while they pick
+ * configurations: an application that owns all device memory through its own
+ * pool, or one that is capturing work into a CUDA graph (cudaMalloc cannot be
+ * captured).  X (n x n_in, row-major) and y (n) are DEVICE pointers the caller
+ * owns; the work is enqueued on `cuda_stream` (a cudaStream_t, NULL for the
+ * default stream) and this call does not wait for it.
+ *   - The activations live in one fixed 2 MiB array compiled into libots
+ *     (every GPU that loads the library holds it until the process exits):
+ *     at most 4096 rows per call, and every layer at most 64 wide; larger
+ *     requests are rejected with OTS_ERR_INVALID_ARGUMENT / UNSUPPORTED.
+ *   - The first call on each device looks up that array's device address
+ *     (cudaGetSymbolAddress) with the model's device current; make that first
+ *     call before any stream capture.
+ *   - All calls share the array: calls whose work overlaps on the GPU race
+ *     (serialise them on one stream).  Each call overwrites what it reads,
+ *     so nothing carries over from the previous call.
+ *   - The model's device must be the current device. */
+ots_status ots_mlp_predict_noalloc(const ots_mlp* model, const float* X, int32_t n, float* y,
+                                   void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif
