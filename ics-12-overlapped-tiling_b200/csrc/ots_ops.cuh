@@ -51,6 +51,35 @@ struct OpArgs {
 
 OTS_HD float sq(float v) { return v * v; }
 
+#if defined(__CUDACC__)
+// Packed FP32 (sm_100 add/sub/mul .f32x2): two IEEE round-to-nearest
+// operations per instruction, so results equal the scalar ones bit for bit.
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+  float2 r;
+  asm("{.reg .b64 p, q, d; mov.b64 p, {%2,%3}; mov.b64 q, {%4,%5}; add.rn.f32x2 d, p, q;"
+      " mov.b64 {%0,%1}, d;}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+  float2 r;
+  asm("{.reg .b64 p, q, d; mov.b64 p, {%2,%3}; mov.b64 q, {%4,%5}; sub.rn.f32x2 d, p, q;"
+      " mov.b64 {%0,%1}, d;}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+  float2 r;
+  asm("{.reg .b64 p, q, d; mov.b64 p, {%2,%3}; mov.b64 q, {%4,%5}; mul.rn.f32x2 d, p, q;"
+      " mov.b64 {%0,%1}, d;}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+#endif
+
 // ---------------------------------------------------------------- 1D ----
 
 // opencl/jacobi-1d/jacobi-1d.cpp:635-637
@@ -234,6 +263,21 @@ struct OpJacobi3D {
                                                float zm, float zp, float, const OpArgs& p) {
     return p.coef * (xm + c + xp + ym + yp + zm + zp);
   }
+  // Two neighbouring cells at once with packed FP32, same operation order.
+  static constexpr bool PACKED = true;
+#if defined(__CUDACC__)
+  __device__ __forceinline__ static float2 star2(float2 xm, float2 c, float2 xp, float2 ym,
+                                                 float2 yp, float2 zm, float2 zp, float2,
+                                                 const OpArgs& p) {
+    float2 s = add2(xm, c);
+    s = add2(s, xp);
+    s = add2(s, ym);
+    s = add2(s, yp);
+    s = add2(s, zm);
+    s = add2(s, zp);
+    return mul2(make_float2(p.coef, p.coef), s);
+  }
+#endif
 };
 
 // Reference: opencl/poisson-3d/poisson-3d.cpp:280-293, 26c - (26 neighbours,
@@ -271,6 +315,15 @@ struct OpPoisson3D {
     float s = xm + xp + ym + yp + zm + zp;
     return (s - p.h2 * f) * (1.0f / 6.0f);
   }
+  // Scalar only: with packed FP32 the h^2 f product and the subtraction were
+  // observed to round once (as a fused multiply-add) in rare cells.
+  static constexpr bool PACKED = false;
+#if defined(__CUDACC__)
+  __device__ __forceinline__ static float2 star2(float2, float2, float2, float2, float2,
+                                                 float2, float2, float2, const OpArgs&) {
+    return make_float2(0.0f, 0.0f);
+  }
+#endif
 };
 
 // opencl/gradient-3d/gradient-3d.cpp:305-307
@@ -290,6 +343,13 @@ struct OpGradient3D {
     return c + ots_rsqrt(0.0001f + sq(c - xm) + sq(c - xp) + sq(c - ym) + sq(c - yp) +
                       sq(c - zm) + sq(c - zp));
   }
+  static constexpr bool PACKED = false;  // 1/sqrt has no packed form
+#if defined(__CUDACC__)
+  __device__ __forceinline__ static float2 star2(float2, float2, float2, float2, float2, float2,
+                                                 float2, float2, const OpArgs&) {
+    return make_float2(0.0f, 0.0f);
+  }
+#endif
 };
 
 // opencl/cs-3d/cs-3d.cpp:161-163 constants, :284-308 arithmetic with y+1 as

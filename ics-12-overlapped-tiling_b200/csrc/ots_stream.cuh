@@ -45,7 +45,10 @@ struct StreamParams {
   OpArgs op;
 };
 
-constexpr int kStreamStages = 4;  // ring depth; lookahead = stages - 2
+#ifndef OTS_STREAM_STAGES
+#define OTS_STREAM_STAGES 4
+#endif
+constexpr int kStreamStages = OTS_STREAM_STAGES;  // ring depth (power of 2); lookahead = stages - 2
 constexpr unsigned kWaitLimit = 1u << 24;
 constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s
 
@@ -130,6 +133,13 @@ __host__ __device__ inline size_t stream_smem_bytes(int T, int TX, int TY) {
 template <int T, int E>
 struct StreamThreads {
   static constexpr int kMax = (T * E >= 8) ? 256 : 512;
+};
+
+// Packed FP32 pairs cut the issue count but need register pairs; they pay at
+// E >= 4 and cost occupancy (more than 128 registers) below that.
+template <class Op, int E>
+struct StreamPacked {
+  static constexpr bool value = Op::PACKED && E >= 4;
 };
 
 template <int N>
@@ -291,17 +301,42 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
       // level T writes the ring slot of level T-1's oldest plane, which no
       // level needs any more (a scratch slot); levels < T write their own ring
       float (&out)[E][V] = (t < T) ? R[t < T ? t : 0][SN] : R[T - 1][SM];
+      if constexpr (StreamPacked<Op, E>::value) {
+        // cells (0,1) and (2,3) of each row as packed pairs
 #pragma unroll
-      for (int e = 0; e < E; ++e)
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-          const float xm = v > 0 ? R[t - 1][SC][e][v - 1] : lv[e];
-          const float xp = v < V - 1 ? R[t - 1][SC][e][v + 1] : rv[e];
-          const float ym = e > 0 ? R[t - 1][SC][e - 1][v] : tvv[v];
-          const float yp = e < E - 1 ? R[t - 1][SC][e + 1][v] : bvv[v];
-          out[e][v] = Op::star(xm, R[t - 1][SC][e][v], xp, ym, yp, R[t - 1][SM][e][v],
-                               R[t - 1][SN][e][v], Op::NA > 0 ? fa[e][v] : 0.0f, p.op);
+        for (int e = 0; e < E; ++e) {
+          const float(&C)[V] = R[t - 1][SC][e];
+          const float* Y0 = e > 0 ? R[t - 1][SC][e - 1] : tvv;
+          const float* Y1 = e < E - 1 ? R[t - 1][SC][e + 1] : bvv;
+          const float(&M)[V] = R[t - 1][SM][e];
+          const float(&N)[V] = R[t - 1][SN][e];
+          const float2 mid = make_float2(C[1], C[2]);
+          const float2 a = Op::star2(
+              make_float2(lv[e], C[0]), make_float2(C[0], C[1]), mid, make_float2(Y0[0], Y0[1]),
+              make_float2(Y1[0], Y1[1]), make_float2(M[0], M[1]), make_float2(N[0], N[1]),
+              Op::NA > 0 ? make_float2(fa[e][0], fa[e][1]) : make_float2(0.0f, 0.0f), p.op);
+          const float2 b = Op::star2(
+              mid, make_float2(C[2], C[3]), make_float2(C[3], rv[e]), make_float2(Y0[2], Y0[3]),
+              make_float2(Y1[2], Y1[3]), make_float2(M[2], M[3]), make_float2(N[2], N[3]),
+              Op::NA > 0 ? make_float2(fa[e][2], fa[e][3]) : make_float2(0.0f, 0.0f), p.op);
+          out[e][0] = a.x;
+          out[e][1] = a.y;
+          out[e][2] = b.x;
+          out[e][3] = b.y;
         }
+      } else {
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            const float xm = v > 0 ? R[t - 1][SC][e][v - 1] : lv[e];
+            const float xp = v < V - 1 ? R[t - 1][SC][e][v + 1] : rv[e];
+            const float ym = e > 0 ? R[t - 1][SC][e - 1][v] : tvv[v];
+            const float yp = e < E - 1 ? R[t - 1][SC][e + 1][v] : bvv[v];
+            out[e][v] = Op::star(xm, R[t - 1][SC][e][v], xp, ym, yp, R[t - 1][SM][e][v],
+                                 R[t - 1][SN][e][v], Op::NA > 0 ? fa[e][v] : 0.0f, p.op);
+          }
+      }
       if (!(zin && xyall)) {  // domain edge: zero the cells outside
 #pragma unroll
         for (int e = 0; e < E; ++e)
