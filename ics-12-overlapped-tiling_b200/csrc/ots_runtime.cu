@@ -1053,8 +1053,13 @@ ots_status ots_describe(const ots_plan* plan, ots_kv_fn kv, void* user) {
   const int loads = si.pp_loads ? si.pp_loads : (int)(si.r5[0] > 0 ? si.r5[0] : 1);
   const int stores = si.pp_stores ? si.pp_stores : si.ns;
   const int flops = si.pp_flops ? si.pp_flops : (int)si.flops;
-  const int64_t thr = (int64_t)p.block_x * (g.dims >= 2 ? p.block_y : 1) *
-                      (g.dims == 3 ? p.block_z : 1) * p.elements_per_thread;
+  // cells one CTA computes per time level: threads x E for the tile kernel;
+  // the whole streamed column (tile x (z segment + pipeline fill)) for the
+  // stream kernel
+  const bool streamk = g.kernel == OTS_KERNEL_STREAM;
+  const int64_t thr = streamk ? (int64_t)g.comps[0] * g.comps[1] * g.comps[2]
+                              : (int64_t)p.block_x * (g.dims >= 2 ? p.block_y : 1) *
+                                    (g.dims == 3 ? p.block_z : 1) * p.elements_per_thread;
   const int64_t total_fp = thr * p.time_tile * flops;
   int64_t useful = (int64_t)p.time_tile * flops;
   for (int a = 0; a < g.dims; ++a) useful *= std::max(0, g.real_per_block[a]);
@@ -1072,8 +1077,11 @@ ots_status ots_describe(const ots_plan* plan, ots_kv_fn kv, void* user) {
   emit_i("Total FP/Block", total_fp);
   emit_i("Useful FP/Block", useful);
   emit_d("Useful Ratio", total_fp ? (double)useful / (double)total_fp : 0.0);
-  emit_i("Global Loads/Block", thr * loads);
-  emit_i("Global Stores/Block", thr * stores);
+  // the stream kernel reads each cell of its column once (TMA) and writes
+  // its interior once
+  emit_i("Global Loads/Block", streamk ? thr : thr * loads);
+  emit_i("Global Stores/Block", streamk ? useful / std::max<int64_t>(1, (int64_t)p.time_tile * flops)
+                                        : thr * stores);
   emit_i("Shared Loads/Block", thr * loads * (p.time_tile - 1));
   emit_i("Shared Stores/Block", thr * stores * (p.time_tile - 1));
   emit_i("Real Per Block X", g.real_per_block[0]);
