@@ -27,7 +27,9 @@ using TileLaunch = cudaError_t (*)(const StepParams&, dim3, dim3, size_t, cudaSt
 using StreamLaunch = cudaError_t (*)(const CUtensorMap&, const StreamParams&, dim3, dim3, size_t,
                                      cudaStream_t);
 using AttrFn = cudaError_t (*)(cudaFuncAttributes*);
-using OccFn = cudaError_t (*)(int*, int, size_t);
+// stream kernel queries take the cluster flag (the clustered instantiation)
+using StreamAttrFn = cudaError_t (*)(cudaFuncAttributes*, bool);
+using StreamOccFn = cudaError_t (*)(int*, int, size_t, bool);
 
 struct StencilKernels {
   TileLaunch tile[3][kMaxE + 1] = {};  // [E axis][E]
@@ -35,8 +37,8 @@ struct StencilKernels {
   TileLaunch plain = nullptr;
   AttrFn plain_attr = nullptr;
   StreamLaunch stream[kMaxT + 1][3] = {};  // [T][index of E in kStreamEs]
-  AttrFn stream_attr[kMaxT + 1][3] = {};
-  OccFn stream_occ[kMaxT + 1][3] = {};
+  StreamAttrFn stream_attr[kMaxT + 1][3] = {};
+  StreamOccFn stream_occ[kMaxT + 1][3] = {};
   bool has_stream = false;
 };
 
@@ -77,25 +79,50 @@ cudaError_t attr_plain(cudaFuncAttributes* a) {
 template <class Op, int T, int E>
 cudaError_t launch_stream(const CUtensorMap& m, const StreamParams& p, dim3 g, dim3 b,
                           size_t smem, cudaStream_t s) {
+  if (p.cy > 1) {  // thread-block clusters of cy CTAs along grid y
+    static std::atomic<size_t> cached_cl{0};
+    cudaError_t e = ensure_smem(stream_kernel<Op, T, E, true>, smem, cached_cl);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = g;
+    cfg.blockDim = b;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 1;
+    attr[0].val.clusterDim.y = (unsigned)p.cy;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, stream_kernel<Op, T, E, true>, m, p);
+  }
   static std::atomic<size_t> cached{0};
-  cudaError_t e = ensure_smem(stream_kernel<Op, T, E>, smem, cached);
+  cudaError_t e = ensure_smem(stream_kernel<Op, T, E, false>, smem, cached);
   if (e != cudaSuccess) return e;
-  stream_kernel<Op, T, E><<<g, b, smem, s>>>(m, p);
+  stream_kernel<Op, T, E, false><<<g, b, smem, s>>>(m, p);
   return cudaGetLastError();
 }
 
 template <class Op, int T, int E>
-cudaError_t attr_stream(cudaFuncAttributes* a) {
-  return cudaFuncGetAttributes(a, stream_kernel<Op, T, E>);
+cudaError_t attr_stream(cudaFuncAttributes* a, bool cl) {
+  return cl ? cudaFuncGetAttributes(a, stream_kernel<Op, T, E, true>)
+            : cudaFuncGetAttributes(a, stream_kernel<Op, T, E, false>);
+}
+
+template <class Op, int T, int E, bool CL>
+cudaError_t occ_stream_k(int* blocks, int threads, size_t smem) {
+  static std::atomic<size_t> cached{0};
+  cudaError_t e = ensure_smem(stream_kernel<Op, T, E, CL>, smem, cached);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, stream_kernel<Op, T, E, CL>,
+                                                       threads, smem);
 }
 
 template <class Op, int T, int E>
-cudaError_t occ_stream(int* blocks, int threads, size_t smem) {
-  static std::atomic<size_t> cached{0};
-  cudaError_t e = ensure_smem(stream_kernel<Op, T, E>, smem, cached);
-  if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, stream_kernel<Op, T, E>, threads,
-                                                       smem);
+cudaError_t occ_stream(int* blocks, int threads, size_t smem, bool cl) {
+  return cl ? occ_stream_k<Op, T, E, true>(blocks, threads, smem)
+            : occ_stream_k<Op, T, E, false>(blocks, threads, smem);
 }
 
 template <class Op, int EAX, int... Es>

@@ -164,6 +164,7 @@ EncodeTiledFn encode_tiled() {
 
 struct StreamCfg {
   int T = 0, E = 0, eidx = 0, bx = 0, by = 0;
+  int cy = 1;              // CTAs per cluster along y (their tiles stack into one)
   int tx = 0, ty = 0, rpbx = 0, rpby = 0, zseg = 0;
   int nbx = 0, nby = 0, nbz = 0;
   int grid = 0;            // persistent CTAs launched
@@ -208,8 +209,10 @@ ots_status derive(const ots_params* p, ots_geometry* g, const StencilInfo** info
   if (!p) return fail(OTS_ERR_INVALID_ARGUMENT, "params is NULL");
   if (p->stencil < 0 || p->stencil >= OTS_NUM_STENCILS)
     return fail(OTS_ERR_INVALID_ARGUMENT, "unknown stencil id %d", p->stencil);
-  for (int i = 0; i < 7; ++i)
+  for (int i = 0; i < 6; ++i)
     if (p->reserved[i] != 0) return fail(OTS_ERR_INVALID_ARGUMENT, "reserved fields must be 0");
+  if (p->cluster_y < 0 || p->cluster_y > 8)
+    return fail(OTS_ERR_INVALID_ARGUMENT, "cluster_y must be 0..8 (got %d)", p->cluster_y);
   const StencilInfo& si = kInfo[p->stencil];
   if (info_out) *info_out = &si;
   const int d = si.dims;
@@ -334,10 +337,11 @@ ots_status derive_stream(const ots_plan* pl, int T, StreamCfg* c) {
   c->bx = p.block_x;
   c->by = p.block_y;
   const int hx = (T + 3) / 4 * 4, hy = T;
+  c->cy = p.cluster_y > 1 ? p.cluster_y : 1;
   c->tx = 4 * c->bx;
   c->ty = c->E * c->by;
   c->rpbx = c->tx - 2 * hx;
-  c->rpby = c->ty - 2 * hy;
+  c->rpby = c->cy * c->ty - 2 * hy;  // one y halo per cluster tile
   const int maxthr = T * c->E >= 8 ? 256 : 512;
   if (c->bx != 8 && c->bx != 16 && c->bx != 32)
     return fail(OTS_ERR_UNSUPPORTED, "stream kernel block x must be 8, 16 or 32 (got %d)", c->bx);
@@ -355,7 +359,7 @@ ots_status derive_stream(const ots_plan* pl, int T, StreamCfg* c) {
     return fail(OTS_ERR_INVALID_GEOMETRY,
                 "Consistency error! stream tile %d x %d leaves no interior at T=%d", c->tx, c->ty,
                 T);
-  c->smem = ots::stream_smem_bytes(T, c->tx, c->ty);
+  c->smem = ots::stream_smem_bytes(T, c->tx, c->ty, c->cy);
   if (c->smem > pl->smem_optin)
     return fail(OTS_ERR_SMEM_TOO_LARGE,
                 "Not enough local memory for even one block! (%zu > %zu bytes)", c->smem,
@@ -366,14 +370,15 @@ ots_status derive_stream(const ots_plan* pl, int T, StreamCfg* c) {
   int per_sm = 1;
   if (pl->K && pl->K->stream_occ[T][eidx]) {
     int b = 0;
-    if (pl->K->stream_occ[T][eidx](&b, c->bx * c->by, c->smem) == cudaSuccess && b > 0) per_sm = b;
+    if (pl->K->stream_occ[T][eidx](&b, c->bx * c->by, c->smem, c->cy > 1) == cudaSuccess && b > 0)
+      per_sm = b;
   }
   // Grid schedule: (tile, z segment) with tiles fastest.  The segment count
   // trades the T-plane pipeline fill of each segment against whole waves of
   // resident CTAs.
   const int64_t work = (int64_t)c->nbx * c->nby * n;
   const int slots = std::max(1, pl->sm_count) * per_sm;
-  const int xy = c->nbx * c->nby;
+  const int xy = c->nbx * c->nby * c->cy;  // CTAs per z segment
   double best = 1e300;
   int best_seg = n;
   for (int nseg = 1; nseg <= std::max(1, n / std::max(1, 2 * T)); ++nseg) {
@@ -391,6 +396,9 @@ ots_status derive_stream(const ots_plan* pl, int T, StreamCfg* c) {
   c->work = work;
   c->chunk = 0;
   c->grid = xy * c->nbz;
+  if ((int64_t)c->nbz * c->cy > 65535)
+    return fail(OTS_ERR_INVALID_GEOMETRY, "stream grid too large along y (%d segments x %d)",
+                c->nbz, c->cy);
   return OTS_OK;
 }
 
@@ -473,7 +481,7 @@ void fill_geometry_for_kernel(ots_plan* pl) {
   if (g.kernel == OTS_KERNEL_STREAM) {
     const StreamCfg& c = pl->scfg;
     g.comps[0] = c.tx;
-    g.comps[1] = c.ty;
+    g.comps[1] = c.cy * c.ty;  // a cluster's CTAs share one tile
     g.comps[2] = c.zseg + 2 * c.T;
     g.real_per_block[0] = c.rpbx;
     g.real_per_block[1] = c.rpby;
@@ -488,14 +496,14 @@ void fill_geometry_for_kernel(ots_plan* pl) {
     g.shared_bytes = (int64_t)c.smem;
     {
       const double n = pl->geo.real_size;
-      g.useful_ratio = (n * n * n) / ((double)c.tx * c.ty * c.nbx * c.nby *
+      g.useful_ratio = (n * n * n) / ((double)c.tx * c.cy * c.ty * c.nbx * c.nby *
                                       (double)c.nbz * (c.zseg + 2 * c.T));
     }
-    if (pl->K->stream_attr[c.T][c.eidx] && pl->K->stream_attr[c.T][c.eidx](&a) == cudaSuccess)
+    if (pl->K->stream_attr[c.T][c.eidx] && pl->K->stream_attr[c.T][c.eidx](&a, c.cy > 1) == cudaSuccess)
       g.registers = a.numRegs;
     int b = 0;
     if (pl->K->stream_occ[c.T][c.eidx] &&
-        pl->K->stream_occ[c.T][c.eidx](&b, c.bx * c.by, c.smem) == cudaSuccess)
+        pl->K->stream_occ[c.T][c.eidx](&b, c.bx * c.by, c.smem, c.cy > 1) == cudaSuccess)
       g.ctas_per_sm = b;
   } else if (g.kernel == OTS_KERNEL_PLAIN) {
     if (pl->K->plain_attr(&a) == cudaSuccess) g.registers = a.numRegs;
@@ -563,6 +571,7 @@ ots_status enqueue_run(ots_plan* pl, int kernel) {
       sp.work = c.work;
       sp.chunk = c.chunk;
       sp.zseg = c.zseg;
+      sp.cy = c.cy;
       sp.base_step = base;
       sp.err = pl->d_err;
       sp.op = pl->op;
@@ -574,7 +583,7 @@ ots_status enqueue_run(ots_plan* pl, int kernel) {
         ots_status st = make_tmap(pl, c, pl->state[pl->cur][0], &m);
         if (st != OTS_OK) return st;
       }
-      e = pl->K->stream[Tl][c.eidx](m, sp, dim3(c.nbx * c.nby, c.nbz, 1), dim3(c.bx, c.by, 1),
+      e = pl->K->stream[Tl][c.eidx](m, sp, dim3(c.nbx * c.nby, c.nbz * c.cy, 1), dim3(c.bx, c.by, 1),
                                     c.smem, pl->stream);
       pl->cur ^= 1;
     }

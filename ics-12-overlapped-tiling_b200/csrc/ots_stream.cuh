@@ -39,7 +39,8 @@ struct StreamParams {
   int ntx, nty;      // x/y tiles
   int64_t work;      // total output tile-planes = ntx * nty * n2
   int64_t chunk;     // persistent mode: tile-planes per CTA (the last gets fewer)
-  int zseg;          // grid mode (> 0): blockIdx.x = tile, blockIdx.y = z segment
+  int zseg;          // grid mode (> 0): blockIdx.x = tile, blockIdx.y = z segment (x cy)
+  int cy;            // CTAs per cluster along y (grid mode); 0 or 1 = no cluster
   int base_step;     // global step index of this launch's first level
   int* err;          // device error word (bit 0: mbarrier wait timed out)
   OpArgs op;
@@ -109,6 +110,37 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
+// ---- thread-block cluster helpers (distributed shared memory) ----------
+__device__ __forceinline__ unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n"
+               "barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// shared::cluster address of the same shared location in CTA `rank`
+__device__ __forceinline__ uint32_t map_shared(const void* p, unsigned rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
+  return r;
+}
+
+// Asynchronous 16-byte store into another CTA's shared memory; its bytes
+// count against the transaction count of that CTA's mbarrier (the consumer
+// arms the barrier with the bytes it expects and waits on it like on a TMA
+// copy; no fence on the producer side).
+__device__ __forceinline__ void st_async_v4(uint32_t addr, uint32_t bar, float a, float b,
+                                            float c, float d) {
+  asm volatile(
+      "st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.f32 [%0], {%1, %2, %3, %4}, [%5];"
+      ::"r"(addr), "f"(a), "f"(b), "f"(c), "f"(d), "r"(bar)
+      : "memory");
+}
+
 template <int T>
 struct StreamGeom {
   static constexpr int HX = (T + 3) / 4 * 4;  // x halo rounded to 16 bytes (TMA x alignment)
@@ -122,10 +154,20 @@ __host__ __device__ inline int stream_plane_stride(int TX, int TY) {
   return (TX * TY + 31) / 32 * 32;
 }
 
-// Shared bytes: ring + (T-1) double-buffered exchange planes + mbarriers.
-__host__ __device__ inline size_t stream_smem_bytes(int T, int TX, int TY) {
+// Cluster halo rows: 3 rotating slots x T levels x (row from the CTA above,
+// row from the CTA below) x TX cells; only clustered launches carry them.
+constexpr int kHaloSlots = 3;
+__host__ __device__ inline int stream_halo_floats(int T, int TX, int cy) {
+  return cy > 1 ? kHaloSlots * T * 2 * TX : 0;
+}
+
+// Shared bytes: ring + (T-1) double-buffered exchange planes + cluster halo
+// rows + mbarriers (ring stages, and one per halo slot and level).
+__host__ __device__ inline size_t stream_smem_bytes(int T, int TX, int TY, int cy = 1) {
   size_t plane = (size_t)stream_plane_stride(TX, TY) * sizeof(float);
-  return (size_t)kStreamStages * plane + (size_t)(T > 1 ? T - 1 : 0) * 2 * plane + 128;
+  return (size_t)kStreamStages * plane + (size_t)(T > 1 ? T - 1 : 0) * 2 * plane +
+         (size_t)stream_halo_floats(T, TX, cy) * sizeof(float) +
+         (size_t)(kStreamStages + kHaloSlots * T * 2) * 8 + 64;
 }
 
 // Threads per CTA are capped so that the register rings (3 planes of 4E
@@ -157,7 +199,28 @@ struct Phase {
 // mode (zseg == 0): one CTA per resident slot, each taking an equal
 // contiguous chunk of the (tile, plane) work.  Grid mode is the default: the
 // persistent chunks lose the halo reuse in L2.
-template <class Op, int T, int E>
+//
+// Clusters along y (CL = true with p.cy > 1, grid mode only): the cy CTAs of a thread-block
+// cluster (blockIdx.y = segment * cy + rank) stack their TY-row tiles into one
+// tile of cy * TY rows, so the y halo of 2T rows is paid once per cluster, not
+// once per CTA.  At every plane each CTA pushes the first and last rows of
+// each level (0..T-1) into its neighbours' halo slots with st.async, whose
+// bytes complete the transaction count of the neighbour's (slot, level,
+// side) mbarrier.  The edge warp that reads a side arms its barriers with the
+// bytes it expects and waits (bounded) on them one plane later, right before
+// the level that reads the row.  Three rotating slots make the pushes
+// race-free: a push into a slot is issued only after the producer's edge
+// threads have waited for rows the consumer pushed after it finished reading
+// that slot.  The consumer re-arms a slot at the start of plane r for plane
+// r+1's pushes (the slot's previous phase was consumed at plane r-1), before
+// its own pushes of plane r, which the producer waits for before pushing
+// plane r+1: so every arm precedes the bytes it counts.  Plane 0's phase is
+// armed before the cluster barrier that opens the kernel.  Clusters need the
+// grid schedule (one z segment per CTA).  No pushes happen on a segment's last plane, so
+// every push is waited for; a cluster barrier at the start (mbarrier init)
+// and at the end (no CTA leaves while a neighbour may still store into it)
+// brackets the loop, and every CTA of a cluster runs the same plane count.
+template <class Op, int T, int E, bool CL>
 __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
     stream_kernel(const __grid_constant__ CUtensorMap tmap,
                   const __grid_constant__ StreamParams p) {
@@ -168,10 +231,15 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
   const int BX = blockDim.x, BY = blockDim.y;
   const int TX = V * BX, TY = E * BY;
   const int PL = stream_plane_stride(TX, TY);
-  const int rpbx = TX - 2 * HX, rpby = TY - 2 * HY;
+  const int cy = CL ? (p.cy > 1 ? p.cy : 1) : 1;  // CL=false compiles the cluster code out
+  const int crank = cy > 1 ? (int)cluster_rank() : 0;  // == blockIdx.y % cy
+  const int rpbx = TX - 2 * HX, rpby = cy * TY - 2 * HY;
   const int tid = threadIdx.x + BX * threadIdx.y;
   const int XB = NST * PL;  // exchange planes start (floats)
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + XB + (T > 1 ? (T - 1) * 2 * PL : 0));
+  const int HB = XB + (T > 1 ? (T - 1) * 2 * PL : 0);  // cluster halo rows start
+  float* const hb = smem + HB;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + HB + stream_halo_floats(T, TX, cy));
+  uint64_t* hbars = bars + NST;  // [slot][level][side 0 = row from above, 1 = from below]
   const unsigned box_bytes = (unsigned)(TX * TY) * sizeof(float);
   const int n2 = p.L.n2;
 
@@ -181,24 +249,48 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
   const int o_bot = (ly + E < TY ? ly + E : TY - 1) * TX + lx;
   const int o_row0 = ly * TX + lx;
   const bool wx = lx >= HX && lx < HX + rpbx;
+  // cluster neighbours: this thread's first row is the CTA's top row (its y-1
+  // neighbour lives in the CTA above), its last row the CTA's bottom row
+  const bool top_ext = cy > 1 && threadIdx.y == 0 && crank > 0;
+  const bool bot_ext = cy > 1 && threadIdx.y == BY - 1 && crank < cy - 1;
+  const unsigned row_bytes = (unsigned)TX * sizeof(float);  // one pushed row
+  // the first thread of an edge row arms that side's barriers
+  const bool arm_top = top_ext && threadIdx.x == 0;
+  const bool arm_bot = bot_ext && threadIdx.x == 0;
+  // pushes go to the CTA above as its "row from below" (side 1), and to the
+  // CTA below as its "row from above" (side 0); remote addresses are mapped
+  // at push time (edge threads only) to keep them out of the register budget
 
   if (tid == 0) {
     for (int s = 0; s < NST; ++s) mbar_init(&bars[s], 1);
+    if (cy > 1)
+      for (int s = 0; s < kHaloSlots * T * 2; ++s) mbar_init(&hbars[s], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   __syncthreads();
+  if (cy > 1) {
+    // plane 0's halo phase (slot 0) is armed before any neighbour can push
+    for (int l = 0; l < T; ++l) {
+      if (arm_top) mbar_arrive_expect_tx(&hbars[l * 2 + 0], row_bytes);
+      if (arm_bot) mbar_arrive_expect_tx(&hbars[l * 2 + 1], row_bytes);
+    }
+    cluster_sync_all();  // neighbours' barriers exist and are armed before any push
+  }
 
   int64_t pos, pend;
   if (p.zseg > 0) {  // grid mode: neighbouring tiles stream the same planes together
-    pos = (int64_t)blockIdx.x * n2 + (int64_t)blockIdx.y * p.zseg;
-    pend = (int64_t)blockIdx.x * n2 + min(n2, (int)(blockIdx.y + 1) * p.zseg);
+    const int seg = (int)blockIdx.y / cy;
+    pos = (int64_t)blockIdx.x * n2 + (int64_t)seg * p.zseg;
+    pend = (int64_t)blockIdx.x * n2 + min(n2, (seg + 1) * p.zseg);
   } else {
     pos = (int64_t)blockIdx.x * p.chunk;
     pend = pos + p.chunk < p.work ? pos + p.chunk : p.work;
   }
   int rg = 0;  // running plane counter across segments: ring stage and parity
+  int hg = 0;  // running halo-phase counter (pushed planes) across segments
   bool ok = true;
+  bool lost = false;  // a halo wait of this thread timed out (reported at the next plane)
   int fail_r = -1;
   while (ok && pos < pend) {
   const int tile = (int)(pos / n2);
@@ -207,7 +299,7 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
   pos += ze - zs;
   const int tyi = tile / p.ntx, txi = tile - tyi * p.ntx;
   const int tx0 = txi * rpbx - HX;  // multiple of 4 (TMA x alignment)
-  const int ty0 = tyi * rpby - HY;
+  const int ty0 = tyi * rpby - HY + crank * TY;  // this CTA's first row
   const int kb = zs - T, ke = ze + T - 1, nit = ke - kb + 1;
   const int gx = tx0 + lx, gy = ty0 + ly;
   unsigned xyin = 0;
@@ -249,9 +341,25 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
     const int g = rg + r;  // running plane index: ring stage and phase parity
     const int st = g & (NST - 1);
     const bool to = !mbar_wait_bounded(&bars[st], (g / NST) & 1, p.err);
-    if (__syncthreads_or(to)) {
+    // cluster halo: the neighbours' rows of plane r-1 (slot of phase hg+r-1)
+    const int hr = (hg + r + kHaloSlots - 1) % kHaloSlots;
+    const unsigned hpar = (unsigned)((hg + r - 1) / kHaloSlots) & 1u;
+    if (__syncthreads_or(to || lost)) {
       fail_r = g;
       return false;
+    }
+    // arm the next plane's halo slot: its previous phase (plane r-2) was
+    // consumed by this edge warp during plane r-1; the warp's own pushes of
+    // this plane follow the arm
+    if (cy > 1) {
+      if (r + 2 < nit) {
+        uint64_t* const hn = &hbars[((hg + r + 1) % kHaloSlots) * T * 2];
+        for (int l = 0; l < T; ++l) {
+          if (arm_top) mbar_arrive_expect_tx(&hn[l * 2 + 0], row_bytes);
+          if (arm_bot) mbar_arrive_expect_tx(&hn[l * 2 + 1], row_bytes);
+        }
+      }
+      __syncwarp();
     }
     if (tid == 0 && r + LA < nit) {
       const int s2 = (g + LA) & (NST - 1);
@@ -265,6 +373,13 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
       const float4 a = *reinterpret_cast<const float4*>(smem + pk + o_row0 + e * TX);
       R[0][SN][e][0] = a.x; R[0][SN][e][1] = a.y; R[0][SN][e][2] = a.z; R[0][SN][e][3] = a.w;
     }
+    // cluster pushes of this plane (none on the segment's last plane: no
+    // neighbour reads them), into slot hw; byte offsets into the remote rows
+    const bool push = cy > 1 && r + 1 < nit;
+    const int hw = (hg + r) % kHaloSlots;
+    float* const hwrow = hb + hw * T * 2 * TX + lx;       // level t at + t*2*TX (+TX: side 1)
+    const float* const hrow = hb + hr * T * 2 * TX + lx;  // level t-1 at + (t-1)*2*TX
+
     const int pc0 = ((g + NST - 1) & (NST - 1)) * PL;   // input plane k-1 (level 1 centre)
     const int xr = XB + ((r - 1) & 1) * PL;              // exchange planes of iteration r-1
     const int xw = XB + (r & 1) * PL;                    // exchange planes of iteration r
@@ -272,8 +387,28 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
     for (int t = 1; t <= T; ++t) {
       const int q = k - t;
       const int cp = (t == 1) ? pc0 : xr + (t - 2) * 2 * PL;
-      const float4 tv = *reinterpret_cast<const float4*>(smem + cp + o_top);
-      const float4 bv = *reinterpret_cast<const float4*>(smem + cp + o_bot);
+      if (r > 0 && !lost) {  // neighbour rows of level t-1, plane r-1
+        if (top_ext) lost = !mbar_wait_bounded(&hbars[(hr * T + t - 1) * 2 + 0], hpar, p.err);
+        if (bot_ext && !lost)
+          lost = !mbar_wait_bounded(&hbars[(hr * T + t - 1) * 2 + 1], hpar, p.err);
+      }
+      const float* const tp = top_ext ? hrow + (t - 1) * 2 * TX : smem + cp + o_top;
+      const float* const bp = bot_ext ? hrow + (t - 1) * 2 * TX + TX : smem + cp + o_bot;
+      const float4 tv = *reinterpret_cast<const float4*>(tp);
+      const float4 bv = *reinterpret_cast<const float4*>(bp);
+      if (t == 1) {
+        // level-0 rows of this plane, pushed only after this thread read its
+        // slot of plane r-1: a producer that has waited for this push knows
+        // the slot it will overwrite next is no longer read
+        if (push && top_ext)
+          st_async_v4(map_shared(hwrow + TX, crank - 1),
+                      map_shared(&hbars[(hw * T) * 2 + 1], crank - 1),
+                      R[0][SN][0][0], R[0][SN][0][1], R[0][SN][0][2], R[0][SN][0][3]);
+        if (push && bot_ext)
+          st_async_v4(map_shared(hwrow, crank + 1), map_shared(&hbars[(hw * T) * 2 + 0], crank + 1),
+                      R[0][SN][E - 1][0], R[0][SN][E - 1][1], R[0][SN][E - 1][2],
+                      R[0][SN][E - 1][3]);
+      }
       float lv[E], rv[E];
 #pragma unroll
       for (int e = 0; e < E; ++e) {
@@ -353,11 +488,19 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
         if (E > 1)
           *reinterpret_cast<float4*>(smem + xb + o_row0 + (E - 1) * TX) =
               make_float4(out[E - 1][0], out[E - 1][1], out[E - 1][2], out[E - 1][3]);
+        if (push && top_ext)
+          st_async_v4(map_shared(hwrow + t * 2 * TX + TX, crank - 1),
+                      map_shared(&hbars[(hw * T + t) * 2 + 1], crank - 1), out[0][0], out[0][1], out[0][2],
+                      out[0][3]);
+        if (push && bot_ext)
+          st_async_v4(map_shared(hwrow + t * 2 * TX, crank + 1),
+                      map_shared(&hbars[(hw * T + t) * 2 + 0], crank + 1), out[E - 1][0], out[E - 1][1],
+                      out[E - 1][2], out[E - 1][3]);
       } else if (q >= zs && q < ze && wx) {
         float* dst = obase + (int64_t)q * p.L.sz;
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-          const int yy = ly + e;
+          const int yy = crank * TY + ly + e;  // row within the (cluster) tile
           if (yy < HY || yy >= HY + rpby) continue;
           const unsigned m = (xyin >> (e * V)) & 0xF;
           if (m == 0xF) {
@@ -382,7 +525,14 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
   }
   if (ok && r < nit) ok = step(Phase<0>{}, r++);
   if (ok && r < nit) ok = step(Phase<1>{}, r++);
-  if (ok) rg += nit;
+  if (ok && cy > 1 && __syncthreads_or(lost)) {  // a halo wait of the last plane timed out
+    ok = false;
+    fail_r = rg + nit;  // every copy of the segment was consumed: nothing to drain
+  }
+  if (ok) {
+    rg += nit;
+    hg += nit - 1;
+  }
   if (!ok) {
     if (tid == 0) {
       atomicOr(p.err, 1);
@@ -394,6 +544,18 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
     __syncthreads();
   }
   }  // segments
+  // no CTA of a cluster leaves while a neighbour may still push into it: on
+  // the normal path every push was waited for; after a failure the pushes
+  // already issued land within microseconds, so a failed cluster lingers
+  // 20 us past the barrier before its shared memory is released
+  if (cy > 1) {
+    cluster_sync_all();
+    if (!ok) {
+      const uint64_t t0 = global_ns();
+      while (global_ns() - t0 < 20000ull) {
+      }
+    }
+  }
 }
 
 }  // namespace ots

@@ -101,9 +101,16 @@ def sweep(stencil, n, steps, space, engine=ENGINE_NATIVE, reps=3, log=None, devi
     return out
 
 
-def stream_space(Ts, bxs, bys, Es):
-    return [dict(kernel="stream", T=T, bx=bx, by=by, bz=1, E=E)
-            for T, bx, by, E in itertools.product(Ts, bxs, bys, Es)]
+def stream_space(Ts, bxs, bys, Es, cys=(1,)):
+    """Stream-kernel configurations; cy > 1 stacks cy CTAs along y in one
+    thread-block cluster sharing a tile (cy = 1 is recorded without the key)."""
+    out = []
+    for T, bx, by, E, cy in itertools.product(Ts, bxs, bys, Es, cys):
+        c = dict(kernel="stream", T=T, bx=bx, by=by, bz=1, E=E)
+        if cy > 1:
+            c["cy"] = cy
+        out.append(c)
+    return out
 
 
 def tile_space(Ts, bxs, bys, bzs, Es):
@@ -128,12 +135,13 @@ def main(argv=None):
     ap.add_argument("--by", default="4,8,16")
     ap.add_argument("--bz", default="1")
     ap.add_argument("--E", default="1,2,4")
+    ap.add_argument("--cy", default="1", help="stream kernel: CTAs per cluster along y")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--out")
     a = ap.parse_args(argv)
     eng = ENGINE_NATIVE if a.engine == "native" else ENGINE_COMPAT
     if a.kernel == "stream":
-        space = stream_space(expand(a.T), expand(a.bx), expand(a.by), expand(a.E))
+        space = stream_space(expand(a.T), expand(a.bx), expand(a.by), expand(a.E), expand(a.cy))
     elif a.kernel == "plain":
         space = [dict(kernel="plain", T=1, bx=32, by=8, bz=1, E=1)]
     else:
@@ -141,9 +149,9 @@ def main(argv=None):
 
     def log(r):
         if r["status"] == "ok":
-            print("%-7s T=%d b=%dx%dx%d E=%d  %8.1f GUpd/s  regs=%d smem=%d" % (
-                r["kernel"], r["T"], r["bx"], r["by"], r["bz"], r["E"], r["gupdates"],
-                r["registers"], r["shared_bytes"]), flush=True)
+            print("%-7s T=%d b=%dx%dx%d E=%d cy=%d  %8.1f GUpd/s  regs=%d smem=%d" % (
+                r["kernel"], r["T"], r["bx"], r["by"], r["bz"], r["E"], r.get("cy", 1),
+                r["gupdates"], r["registers"], r["shared_bytes"]), flush=True)
 
     recs = sweep(a.stencil, a.n, a.t, space, engine=eng, reps=a.reps, log=log)
     b = best(recs)

@@ -115,7 +115,12 @@ typedef struct ots_params {
   float coef;                  /* averaging weight; 0 = the stencil's default */
   float h2;                    /* Poisson h^2; 0 = 1/(real_size-1)^2 */
   int32_t device;              /* CUDA device ordinal */
-  int32_t reserved[7];         /* must be zero */
+  int32_t cluster_y;           /* stream kernel: CTAs per thread-block cluster
+                                  stacked along y (1..8; 0 or 1 = none).  The
+                                  cluster shares one tile of cluster_y * block_y
+                                  * E rows, so the 2T-row y halo is recomputed
+                                  once per cluster instead of once per CTA. */
+  int32_t reserved[6];         /* must be zero */
 } ots_params;
 
 /* Derived values: the reference's GeneratorParams fields plus what the

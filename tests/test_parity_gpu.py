@@ -118,6 +118,29 @@ def test_stream_kernel_matches_oracle(st, T, E):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("cy", [2, 3, 4, 8])
+@pytest.mark.parametrize("st,T,E,bx,by", [
+    ("jacobi-3d", 1, 2, 16, 8),
+    ("jacobi-3d", 3, 2, 8, 16),
+    ("jacobi-3d", 2, 4, 16, 4),
+    ("jacobi-3d", 4, 1, 32, 8),
+    ("poisson-3d", 3, 2, 16, 4),
+    ("gradient-3d", 2, 1, 8, 8),
+])
+def test_stream_cluster_matches_oracle(cy, st, T, E, bx, by):
+    # y-clustered tiles: rows cross CTA boundaries through distributed shared
+    # memory; n not a multiple of the cluster tile, several z segments
+    run_and_check(st, 70, 2 * T + 1, T=T, bx=bx, by=by, bz=1, E=E, kernel="stream", cy=cy)
+
+
+@pytest.mark.gpu
+def test_stream_cluster_block_one_row_and_partial():
+    # by = 1: each thread is both the top and the bottom row of its CTA
+    run_and_check("jacobi-3d", 45, 7, T=2, bx=32, by=1, bz=1, E=4, kernel="stream", cy=4)
+    run_and_check("jacobi-3d", 133, 10, T=3, bx=16, by=8, bz=1, E=2, kernel="stream", cy=3)
+
+
+@pytest.mark.gpu
 def test_stream_kernel_partial_tiles_and_segments():
     # n not a multiple of the tile interior, more steps than one launch
     run_and_check("jacobi-3d", 133, 10, T=4, bx=32, by=6, bz=1, E=2, kernel="stream")
@@ -205,6 +228,23 @@ def test_errors_are_statuses_not_crashes():
     with pytest.raises(ots.OtsError) as ei:
         ots.Plan("jacobi-2d", 64, 4, device=999)
     assert ei.value.status_name == "INVALID_ARGUMENT"
+
+
+@pytest.mark.gpu
+def test_full_size_jacobi_3d_cluster_tiled_equals_plain():
+    """512^3 x 100 steps with y-clustered stream tiles (4 CTAs per cluster):
+    identical bits to the plain one-step kernel."""
+    n, steps = 512, 100
+    with ots.Plan("jacobi-3d", n, steps, T=3, bx=16, by=8, bz=1, E=2, kernel="stream",
+                  cy=4) as plan:
+        state, _ = plan.fill_reference(seed=99)
+        plan.upload(state)
+        plan.run("stream")
+        a = plan.download_interior()[0]
+        plan.upload(state)
+        plan.run("plain")
+        b = plan.download_interior()[0]
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
 
 
 @pytest.mark.gpu
