@@ -43,7 +43,7 @@ void usage(const char* prog) {
           "  -f, --load-kernel FILE       (rejected: kernels are compiled ahead of time)\n"
           "  -w, --save-kernel FILE       Save a description of the chosen kernel\n"
           "  -v, --verify                 Verify results against a CPU sweep\n"
-          "  -c, --dump-clocks BOOL       Accepted for compatibility\n"
+          "  -c, --dump-clocks BOOL       Dump per-warp phase clocks (tile kernel) to stderr\n"
           "  -b, --break-threads          Accepted for compatibility\n"
           "      --time-only WHAT         Accepted for compatibility (gmem, instr, smem)\n"
           "      --stencil NAME           Stencil (default: from the program name)\n"
@@ -150,7 +150,7 @@ int main(int argc, char** argv) {
   p.kernel = OTS_KERNEL_AUTO;
   p.variant = -1;
   unsigned seed = 123456;  // srand(123456), opencl/jacobi-2d/jacobi-2d.cpp:561
-  bool verify = false, plain = false, bx_set = false, by_set = false;
+  bool verify = false, plain = false, bx_set = false, by_set = false, dump_clocks = false;
   std::string save_kernel, load_kernel;
 
   for (int i = 1; i < argc; ++i) {
@@ -188,7 +188,7 @@ int main(int argc, char** argv) {
     else if (a == "-f" || a == "--load-kernel") load_kernel = next();
     else if (a == "-w" || a == "--save-kernel") save_kernel = next();
     else if (a == "-v" || a == "--verify") verify = true;
-    else if (a == "-c" || a == "--dump-clocks") (void)parse_bool(next());
+    else if (a == "-c" || a == "--dump-clocks") dump_clocks = parse_bool(next());
     else if (a == "-b" || a == "--break-threads") {
     } else if (a == "--time-only") (void)next();
     else if (a == "--stencil") stencil = ots_stencil_from_name(next());
@@ -278,8 +278,25 @@ int main(int argc, char** argv) {
   for (auto& v : state) sp.push_back(v.data());
   for (auto& v : aux) ap.push_back(v.data());
   st = ots_upload(plan, sp.data(), ap.empty() ? nullptr : ap.data());
+  if (st == OTS_OK && dump_clocks && ots_plan_enable_clocks(plan, 1) != OTS_OK)
+    fprintf(stderr, "warning: clock dump unavailable: %s\n", ots_last_error());
   ots_timing tm{};
   if (st == OTS_OK) st = ots_run(plan, OTS_KERNEL_AUTO, &tm);
+  if (st == OTS_OK && dump_clocks) {
+    // opencl/jacobi-2d/jacobi-2d.cpp:957-996: the warps that ran on SM 1
+    int64_t n = 0;
+    if (ots_plan_clock_records(plan, nullptr, 0, &n) == OTS_OK && n > 0) {
+      std::vector<ots_clock_record> recs((size_t)n);
+      if (ots_plan_clock_records(plan, recs.data(), n, &n) == OTS_OK) {
+        fprintf(stderr, "bx,by,warp,sm,clock0,clock1,clock2,clock3,clock4,\n");
+        for (const ots_clock_record& r : recs)
+          if (r.sm == 1)
+            fprintf(stderr, "%u,%u,%u,%u,%u,%u,%u,%u,%u,\n", r.block_x,
+                    r.block_y + r.block_z * (uint32_t)g.num_blocks[1], r.warp, r.sm, r.clock[0],
+                    r.clock[1], r.clock[2], r.clock[3], r.clock[4]);
+      }
+    }
+  }
   std::vector<float*> dp;
   for (auto& v : state) dp.push_back(v.data());
   if (st == OTS_OK) st = ots_download(plan, dp.data());

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <vector>
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
@@ -191,6 +192,10 @@ struct ots_plan {
   float* aux[2] = {};
   int cur = 0;
   int* d_err = nullptr;
+  // -c clock recording (tile kernel): kClockWords per warp of the last launch
+  unsigned* d_clocks = nullptr;
+  int64_t clock_warps = 0;
+  bool clocks_valid = false;  // the last run used the tile kernel
   ots::OpArgs op{};
   CUtensorMap tmap[2];  // stream kernel: field 0 of state buffer 0 / 1
   bool tmap_ok = false;
@@ -592,10 +597,12 @@ ots_status enqueue_run(ots_plan* pl, int kernel) {
     auto fn = pl->K->tile[pl->geo.e_axis][pl->prm.elements_per_thread];
     for (int base = 0; base < S && e == cudaSuccess; base += T) {
       ots::StepParams sp = step_params(pl, pl->cur, base, T);
+      sp.clocks = pl->d_clocks;  // each launch overwrites: the last one stays
       e = fn(sp, pl->tile_grid, pl->tile_block, pl->tile_smem, pl->stream);
       pl->cur ^= 1;
     }
   }
+  pl->clocks_valid = pl->d_clocks && kernel == OTS_KERNEL_TILE;
   if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
   return OTS_OK;
 }
@@ -670,6 +677,7 @@ void free_plan(ots_plan* pl) {
   for (int a = 0; a < 2; ++a)
     if (pl->aux[a]) cudaFree(pl->aux[a]);
   if (pl->d_err) cudaFree(pl->d_err);
+  if (pl->d_clocks) cudaFree(pl->d_clocks);
   if (pl->ev0) cudaEventDestroy(pl->ev0);
   if (pl->ev1) cudaEventDestroy(pl->ev1);
   if (pl->stream) cudaStreamDestroy(pl->stream);
@@ -734,6 +742,15 @@ int32_t ots_stencil_num_fields(int32_t s) {
 }
 int32_t ots_stencil_num_aux(int32_t s) {
   return (s >= 0 && s < OTS_NUM_STENCILS) ? kInfo[s].na : 0;
+}
+
+ots_status ots_stencil_model_constants(int32_t s, double out[8]) {
+  if (s < 0 || s >= OTS_NUM_STENCILS) return fail(OTS_ERR_INVALID_ARGUMENT, "unknown stencil id %d", s);
+  if (!out) return fail(OTS_ERR_INVALID_ARGUMENT, "out is NULL");
+  if (kInfo[s].r5[0] < 0)
+    return fail(OTS_ERR_UNSUPPORTED, "the %s runner prints no model constants", kInfo[s].name);
+  for (int i = 0; i < 8; ++i) out[i] = kInfo[s].r5[i];
+  return OTS_OK;
 }
 
 ots_status ots_fill_reference(int32_t dims, int32_t P, int32_t padding, int32_t real_size,
@@ -1022,6 +1039,55 @@ ots_status ots_plan_device_aux(const ots_plan* plan, int32_t field, float** ptr)
   if (!plan || !ptr || field < 0 || field >= plan->info->na)
     return fail(OTS_ERR_INVALID_ARGUMENT, "bad aux field request");
   *ptr = plan->aux[field];
+  return OTS_OK;
+}
+
+ots_status ots_plan_enable_clocks(ots_plan* pl, int32_t enable) {
+  if (!pl) return fail(OTS_ERR_INVALID_ARGUMENT, "NULL plan");
+  OTS_CUDA(cudaSetDevice(pl->device), "cudaSetDevice");
+  if (pl->d_clocks) {
+    OTS_CUDA(cudaStreamSynchronize(pl->stream), "synchronize");
+    cudaFree(pl->d_clocks);
+    pl->d_clocks = nullptr;
+    pl->clock_warps = 0;
+    pl->clocks_valid = false;
+  }
+  if (!enable) return OTS_OK;
+  const int64_t blocks = (int64_t)pl->tile_grid.x * pl->tile_grid.y * pl->tile_grid.z;
+  const int64_t threads = (int64_t)pl->tile_block.x * pl->tile_block.y * pl->tile_block.z;
+  if (blocks <= 0 || threads <= 0)
+    return fail(OTS_ERR_UNSUPPORTED, "clock recording needs the tile kernel's launch shape");
+  pl->clock_warps = blocks * ((threads + 31) / 32);
+  const size_t bytes = (size_t)pl->clock_warps * ots::kClockWords * sizeof(unsigned);
+  OTS_CUDA(cudaMalloc(&pl->d_clocks, bytes), "cudaMalloc clocks");
+  OTS_CUDA(cudaMemset(pl->d_clocks, 0, bytes), "cudaMemset clocks");
+  return OTS_OK;
+}
+
+ots_status ots_plan_clock_records(ots_plan* pl, ots_clock_record* out, int64_t capacity,
+                                  int64_t* count) {
+  if (!pl || !count) return fail(OTS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (!pl->d_clocks) return fail(OTS_ERR_INVALID_ARGUMENT, "clock recording is off");
+  *count = pl->clocks_valid ? pl->clock_warps : 0;
+  if (!pl->clocks_valid || !out || capacity <= 0) return OTS_OK;
+  OTS_CUDA(cudaSetDevice(pl->device), "cudaSetDevice");
+  std::vector<unsigned> raw((size_t)pl->clock_warps * ots::kClockWords);
+  OTS_CUDA(cudaMemcpyAsync(raw.data(), pl->d_clocks, raw.size() * sizeof(unsigned),
+                           cudaMemcpyDeviceToHost, pl->stream),
+           "read clocks");
+  OTS_CUDA(cudaStreamSynchronize(pl->stream), "synchronize");
+  const int64_t wpb = ((int64_t)pl->tile_block.x * pl->tile_block.y * pl->tile_block.z + 31) / 32;
+  const int64_t n = std::min<int64_t>(capacity, pl->clock_warps);
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t blk = i / wpb;
+    ots_clock_record& r = out[i];
+    r.block_x = (uint32_t)(blk % pl->tile_grid.x);
+    r.block_y = (uint32_t)((blk / pl->tile_grid.x) % pl->tile_grid.y);
+    r.block_z = (uint32_t)(blk / ((int64_t)pl->tile_grid.x * pl->tile_grid.y));
+    r.warp = (uint32_t)(i % wpb);
+    r.sm = raw[(size_t)i * ots::kClockWords];
+    for (int c = 0; c < 5; ++c) r.clock[c] = raw[(size_t)i * ots::kClockWords + 1 + c];
+  }
   return OTS_OK;
 }
 

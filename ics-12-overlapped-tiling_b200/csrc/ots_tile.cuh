@@ -43,7 +43,28 @@ struct StepParams {
   int base_step;     // global index of this launch's first step
   int phase_limit;   // 0 full, 1/2/3 partial kernels (reference -p)
   OpArgs op;
+  // -c: per warp {smid, %clock at entry, after set-up, after the global load
+  // and first step, after the in-tile steps, after the write-back}, indexed
+  // by linear block x warps per block; nullptr = off
+  unsigned* clocks;
 };
+
+constexpr int kClockWords = 6;
+
+// Lane 0 of each warp stores its clock record (the reference keeps the
+// records of SM 1 only, opencl/jacobi-2d/jacobi-2d.cpp:488-508; all SMs are
+// kept here and the host filters).
+__device__ __forceinline__ void clock_store(const StepParams& p, int tid, int nth,
+                                            const unsigned (&ck)[5]) {
+  if (!p.clocks || (tid & 31) != 0) return;
+  unsigned sm;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
+  const unsigned blk = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  unsigned* r = p.clocks + ((size_t)blk * ((nth + 31) / 32) + (tid >> 5)) * kClockWords;
+  r[0] = sm;
+#pragma unroll
+  for (int i = 0; i < 5; ++i) r[1 + i] = ck[i];
+}
 
 __device__ __forceinline__ bool in_domain(const Layout& L, int x, int y, int z) {
   return (unsigned)x < (unsigned)L.n0 && (unsigned)y < (unsigned)L.n1 &&
@@ -124,7 +145,13 @@ __device__ __forceinline__ void tile_body(const StepParams& p, int bix, int biy,
   const int oz = biz * p.rpb[2] - RZ * (T - 1);
   const int tid = tx + bx * (ty + by * tz);
   const int nth = bx * by * bz;
-  if (p.phase_limit == 1) return;
+  unsigned ck[5] = {0, 0, 0, 0, 0};
+  if (p.clocks) ck[0] = (unsigned)clock();
+  if (p.clocks) ck[1] = (unsigned)clock();  // set-up (index arithmetic) done
+  if (p.phase_limit == 1) {
+    clock_store(p, tid, nth, ck);
+    return;
+  }
 
   float* cur = smem;
   float* nxt = smem + NS * Lvol;
@@ -187,9 +214,17 @@ __device__ __forceinline__ void tile_body(const StepParams& p, int bix, int biy,
     float* t = cur;
     cur = nxt;
     nxt = t;
-    if (p.phase_limit == 2) return;
+    if (s == 0 && p.clocks) ck[2] = (unsigned)clock();  // global load + first step
+    if (p.phase_limit == 2) {
+      clock_store(p, tid, nth, ck);
+      return;
+    }
   }
-  if (p.phase_limit == 3) return;
+  if (p.clocks) ck[3] = (unsigned)clock();  // the in-tile steps
+  if (p.phase_limit == 3) {
+    clock_store(p, tid, nth, ck);
+    return;
+  }
 
   // Interior write-back: comps coordinate in [r(T-1), r(T-1) + rpb) per axis.
 #pragma unroll
@@ -203,6 +238,10 @@ __device__ __forceinline__ void tile_body(const StepParams& p, int bix, int biy,
 #pragma unroll
       for (int f = 0; f < NS; ++f) p.out[f][gi] = cur[f * Lvol + sidx[e]];
     }
+  }
+  if (p.clocks) {
+    ck[4] = (unsigned)clock();  // write-back
+    clock_store(p, tid, nth, ck);
   }
 }
 

@@ -114,6 +114,8 @@ def lib():
     for fn in ("ots_stencil_dims", "ots_stencil_num_fields", "ots_stencil_num_aux"):
         getattr(L, fn).argtypes = [ctypes.c_int32]
         getattr(L, fn).restype = ctypes.c_int32
+    L.ots_stencil_model_constants.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]
+    L.ots_stencil_model_constants.restype = st
     L.ots_fill_reference.argtypes = [ctypes.c_int32] * 4 + [ctypes.c_uint32,
                                                             ctypes.POINTER(_FP), ctypes.c_int32]
     L.ots_fill_reference.restype = st
@@ -145,6 +147,11 @@ def lib():
         getattr(L, fn).restype = st
     L.ots_plan_stream.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
     L.ots_plan_stream.restype = st
+    L.ots_plan_enable_clocks.argtypes = [ctypes.c_void_p, ctypes.c_int32]
+    L.ots_plan_enable_clocks.restype = st
+    L.ots_plan_clock_records.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                         ctypes.POINTER(ctypes.c_int64)]
+    L.ots_plan_clock_records.restype = st
     L.ots_host_register.argtypes = [ctypes.c_void_p, ctypes.c_size_t]
     L.ots_host_register.restype = st
     L.ots_host_unregister.argtypes = [ctypes.c_void_p]
@@ -177,6 +184,22 @@ def make_params(stencil, n, steps, T=1, bx=16, by=16, bz=1, E=1, engine=ENGINE_N
     p.variant, p.phase_limit, p.coef, p.h2, p.device = variant, phase_limit, coef, h2, device
     p.cluster_y = cy
     return p
+
+
+MODEL_CONSTANT_KEYS = ("phase2_global_loads", "phase2_shared_loads", "compute_per_point",
+                       "phase3_shared_loads", "phase4_global_stores", "shared_stores",
+                       "num_fields", "data_size")
+
+
+def model_constants(stencil):
+    """The runner's printed performance-model constants (dict), or None for
+    the runners that print none."""
+    sid = SID[stencil] if isinstance(stencil, str) else int(stencil)
+    out = (ctypes.c_double * 8)()
+    st = lib().ots_stencil_model_constants(sid, out)
+    if st != 0:
+        return None
+    return dict(zip(MODEL_CONSTANT_KEYS, list(out)))
 
 
 def derive_geometry(**kw):
@@ -322,6 +345,24 @@ class Plan:
         p = ctypes.c_void_p()
         check(lib().ots_plan_device_state(self.handle, field, ctypes.byref(p)))
         return p.value
+
+    def enable_clocks(self, enable=True):
+        """Record per-warp phase clocks of tile-kernel launches (-c)."""
+        check(lib().ots_plan_enable_clocks(self.handle, 1 if enable else 0))
+
+    def clock_records(self):
+        """The last tile-kernel launch's records: a structured array with
+        block_x, block_y, block_z, warp, sm and clock[5]."""
+        import numpy as _np
+        dt = _np.dtype([("block_x", "<u4"), ("block_y", "<u4"), ("block_z", "<u4"),
+                        ("warp", "<u4"), ("sm", "<u4"), ("clock", "<u4", (5,))])
+        n = ctypes.c_int64()
+        check(lib().ots_plan_clock_records(self.handle, None, 0, ctypes.byref(n)))
+        out = _np.zeros(n.value, dt)
+        if n.value:
+            check(lib().ots_plan_clock_records(self.handle, out.ctypes.data, n.value,
+                                               ctypes.byref(n)))
+        return out
 
     def stream_ptr(self):
         p = ctypes.c_void_p()

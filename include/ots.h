@@ -179,6 +179,13 @@ int32_t ots_stencil_from_name(const char* name); /* -1 if unknown */
 int32_t ots_stencil_dims(int32_t stencil);
 int32_t ots_stencil_num_fields(int32_t stencil);
 int32_t ots_stencil_num_aux(int32_t stencil);
+/* The performance-model constants the reference runner prints for this
+ * stencil (opencl/jacobi-2d/jacobi-2d.cpp:1029-1036 and the matching lines of
+ * each runner), in the order phase2_global_loads, phase2_shared_loads,
+ * compute_per_point, phase3_shared_loads, phase4_global_stores,
+ * shared_stores, num_fields, data_size.  OTS_ERR_UNSUPPORTED for the runners
+ * that print none (jacobi-1d-5pt, jacobi-1d-7pt, cs-3d).  Needs no GPU. */
+ots_status ots_stencil_model_constants(int32_t stencil, double out[8]);
 
 /* Fill P^d host arrays (state fields then aux fields, as the reference
  * interleaves them per cell) with srand(seed); rand()/(RAND_MAX+1.0f) over
@@ -238,6 +245,21 @@ ots_status ots_describe(const ots_plan* plan, ots_kv_fn kv, void* user);
 ots_status ots_plan_device_state(const ots_plan* plan, int32_t field, float** device_ptr);
 ots_status ots_plan_device_aux(const ots_plan* plan, int32_t field, float** device_ptr);
 ots_status ots_plan_stream(const ots_plan* plan, void** cuda_stream);
+
+/* -c/--dump-clocks (opencl/jacobi-2d/jacobi-2d.cpp:178-204, :484-508,
+ * :957-996): with recording on, every tile-kernel launch stores per warp the
+ * SM id and %clock at five points -- entry, after set-up, after the global
+ * load and first step, after the in-tile steps, after the write-back -- and
+ * the last launch's records stay.  ots_plan_clock_records copies up to
+ * `capacity` of them (block-major, warps in order) and sets *count to the
+ * number available (0 if the last run was not the tile kernel). */
+typedef struct ots_clock_record {
+  uint32_t block_x, block_y, block_z, warp, sm;
+  uint32_t clock[5];
+} ots_clock_record;
+ots_status ots_plan_enable_clocks(ots_plan* plan, int32_t enable);
+ots_status ots_plan_clock_records(ots_plan* plan, ots_clock_record* out, int64_t capacity,
+                                  int64_t* count);
 
 /* Page-lock a caller's host buffer so uploads/downloads run as async DMA. */
 ots_status ots_host_register(void* ptr, size_t bytes);
