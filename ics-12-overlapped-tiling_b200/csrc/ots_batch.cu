@@ -59,9 +59,9 @@ __device__ __forceinline__ void batch_tile(const StepParams& p, int eidx, int tx
   const int by = kBatchThreads / bx;
   const int tx = threadIdx.x % bx, ty = threadIdx.x / bx;
   switch (eidx) {
-    case 0: tile_body<Op, 1, 1, true>(p, txi, tyi, 0, bx, by, 1, tx, ty, 0, smem); break;
-    case 1: tile_body<Op, 2, 1, true>(p, txi, tyi, 0, bx, by, 1, tx, ty, 0, smem); break;
-    default: tile_body<Op, 4, 1, true>(p, txi, tyi, 0, bx, by, 1, tx, ty, 0, smem); break;
+    case 0: tile_body<Op, 1, 1, kLoadCg>(p, txi, tyi, 0, bx, by, 1, tx, ty, 0, smem); break;
+    case 1: tile_body<Op, 2, 1, kLoadCg>(p, txi, tyi, 0, bx, by, 1, tx, ty, 0, smem); break;
+    default: tile_body<Op, 4, 1, kLoadCg>(p, txi, tyi, 0, bx, by, 1, tx, ty, 0, smem); break;
   }
 }
 

@@ -22,6 +22,7 @@ constexpr int kMaxE = 16;       // tile kernel, 1D/2D
 constexpr int kMaxE3 = 8;       // tile kernel, 3D
 constexpr int kMaxT = 8;        // stream kernel levels
 constexpr int kStreamEs[3] = {1, 2, 4};
+constexpr int kTexMaxE = 8;     // texture-path tile kernel (2D, one state field)
 
 using TileLaunch = cudaError_t (*)(const StepParams&, dim3, dim3, size_t, cudaStream_t);
 using StreamLaunch = cudaError_t (*)(const CUtensorMap&, const StreamParams&, dim3, dim3, size_t,
@@ -36,6 +37,8 @@ struct StencilKernels {
   AttrFn tile_attr[3][kMaxE + 1] = {};
   TileLaunch plain = nullptr;
   AttrFn plain_attr = nullptr;
+  TileLaunch tex[kTexMaxE + 1] = {};  // [E]
+  AttrFn tex_attr[kTexMaxE + 1] = {};
   StreamLaunch stream[kMaxT + 1][3] = {};  // [T][index of E in kStreamEs]
   StreamAttrFn stream_attr[kMaxT + 1][3] = {};
   StreamOccFn stream_occ[kMaxT + 1][3] = {};
@@ -63,6 +66,20 @@ cudaError_t launch_tile(const StepParams& p, dim3 g, dim3 b, size_t smem, cudaSt
 template <class Op, int E, int EAX>
 cudaError_t attr_tile(cudaFuncAttributes* a) {
   return cudaFuncGetAttributes(a, tile_kernel<Op, E, EAX>);
+}
+
+template <class Op, int E>
+cudaError_t launch_tex(const StepParams& p, dim3 g, dim3 b, size_t smem, cudaStream_t s) {
+  static std::atomic<size_t> cached{0};
+  cudaError_t e = ensure_smem(tile_tex_kernel<Op, E>, smem, cached);
+  if (e != cudaSuccess) return e;
+  tile_tex_kernel<Op, E><<<g, b, smem, s>>>(p);
+  return cudaGetLastError();
+}
+
+template <class Op, int E>
+cudaError_t attr_tex(cudaFuncAttributes* a) {
+  return cudaFuncGetAttributes(a, tile_tex_kernel<Op, E>);
 }
 
 template <class Op>
@@ -132,6 +149,11 @@ void fill_tile(StencilKernels& k, std::integer_sequence<int, Es...>) {
    ...);
 }
 
+template <class Op, int... Es>
+void fill_tex(StencilKernels& k, std::integer_sequence<int, Es...>) {
+  ((k.tex[Es + 1] = &launch_tex<Op, Es + 1>, k.tex_attr[Es + 1] = &attr_tex<Op, Es + 1>), ...);
+}
+
 template <class Op, int EI, int... Ts>
 void fill_stream_e(StencilKernels& k, std::integer_sequence<int, Ts...>) {
   ((k.stream[Ts + 1][EI] = &launch_stream<Op, Ts + 1, kStreamEs[EI]>,
@@ -145,6 +167,8 @@ StencilKernels make_kernels() {
   StencilKernels k;
   if constexpr (Op::DIMS == 1) fill_tile<Op, 0>(k, std::make_integer_sequence<int, kMaxE>{});
   if constexpr (Op::DIMS == 2) fill_tile<Op, 1>(k, std::make_integer_sequence<int, kMaxE>{});
+  if constexpr (Op::DIMS == 2 && Op::NS == 1)
+    fill_tex<Op>(k, std::make_integer_sequence<int, kTexMaxE>{});
   if constexpr (Op::DIMS == 3) {
     fill_tile<Op, 2>(k, std::make_integer_sequence<int, kMaxE3>{});
     fill_tile<Op, 1>(k, std::make_integer_sequence<int, kMaxE3>{});

@@ -48,7 +48,7 @@ void usage(const char* prog) {
           "      --time-only WHAT         Accepted for compatibility (gmem, instr, smem)\n"
           "      --stencil NAME           Stencil (default: from the program name)\n"
           "      --engine compat|native   Geometry derivation (default compat)\n"
-          "      --kernel auto|tile|stream|plain\n"
+          "      --kernel auto|tile|stream|plain|tex\n"
           "      --variant ref|baseline   Arithmetic variant (default: ref for compat)\n"
           "      --coef X                 Averaging weight (Jacobi stencils)\n"
           "      --seed N                 srand seed for the input fill (default 123456)\n"
@@ -196,7 +196,7 @@ int main(int argc, char** argv) {
     else if (a == "--kernel") {
       const std::string k = next();
       p.kernel = k == "tile" ? OTS_KERNEL_TILE : k == "stream" ? OTS_KERNEL_STREAM
-                 : k == "plain" ? OTS_KERNEL_PLAIN : OTS_KERNEL_AUTO;
+                 : k == "plain" ? OTS_KERNEL_PLAIN : k == "tex" ? OTS_KERNEL_TEX : OTS_KERNEL_AUTO;
     } else if (a == "--variant") p.variant = strcmp(next(), "baseline") == 0 ? OTS_VARIANT_BASELINE : OTS_VARIANT_REF;
     else if (a == "--coef") p.coef = (float)atof(next());
     else if (a == "--seed") seed = (unsigned)strtoul(next(), nullptr, 10);

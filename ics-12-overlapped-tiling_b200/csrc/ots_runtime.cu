@@ -199,6 +199,8 @@ struct ots_plan {
   ots::OpArgs op{};
   CUtensorMap tmap[2];  // stream kernel: field 0 of state buffer 0 / 1
   bool tmap_ok = false;
+  cudaTextureObject_t tex[2] = {0, 0};  // texture kernel: field 0 of state buffer 0 / 1
+  bool tex_ok = false;
   StreamCfg scfg;
   // tile kernel launch shape
   dim3 tile_grid, tile_block;
@@ -230,7 +232,7 @@ ots_status derive(const ots_params* p, ots_geometry* g, const StencilInfo** info
   if (bx < 1 || by < 1 || bz < 1) return fail(OTS_ERR_INVALID_ARGUMENT, "block sizes must be >= 1");
   if (p->engine != OTS_ENGINE_NATIVE && p->engine != OTS_ENGINE_COMPAT)
     return fail(OTS_ERR_INVALID_ARGUMENT, "unknown engine %d", p->engine);
-  if (p->kernel < OTS_KERNEL_AUTO || p->kernel > OTS_KERNEL_PLAIN)
+  if (p->kernel < OTS_KERNEL_AUTO || p->kernel > OTS_KERNEL_TEX)
     return fail(OTS_ERR_INVALID_ARGUMENT, "unknown kernel family %d", p->kernel);
   if (p->variant != OTS_VARIANT_BASELINE && p->variant != OTS_VARIANT_REF)
     return fail(OTS_ERR_INVALID_ARGUMENT, "unknown variant %d", p->variant);
@@ -435,7 +437,47 @@ ots_status resolve_kernel(ots_plan* pl, int requested, int* out) {
                                                                       : OTS_KERNEL_TILE;
   if (k == OTS_KERNEL_STREAM && !star_ok)
     return fail(OTS_ERR_UNSUPPORTED, "stream kernel covers the 3D star stencils only");
+  if (k == OTS_KERNEL_TEX &&
+      (si.dims != 2 || si.ns != 1 || p.elements_per_thread < 1 ||
+       p.elements_per_thread > ots::kTexMaxE || !pl->K->tex[p.elements_per_thread]))
+    return fail(OTS_ERR_UNSUPPORTED,
+                "texture kernel covers 2D single-field stencils with E <= %d", ots::kTexMaxE);
   *out = k;
+  return OTS_OK;
+}
+
+// Texture objects over field 0 of both state buffers (pitch-linear 2D, border
+// addressing: a fetch outside the interior reads 0, the Dirichlet ring).
+ots_status make_textures(ots_plan* pl) {
+  if (pl->tex_ok) return OTS_OK;
+  int align = 0, maxw = 0, maxh = 0;
+  cudaDeviceGetAttribute(&align, cudaDevAttrTexturePitchAlignment, pl->device);
+  cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxTexture2DLinearWidth, pl->device);
+  cudaDeviceGetAttribute(&maxh, cudaDevAttrMaxTexture2DLinearHeight, pl->device);
+  const size_t pitch = (size_t)pl->L.sy * sizeof(float);
+  if (align <= 0 || pitch % (size_t)align != 0 || pl->L.n0 > maxw || pl->L.n1 > maxh)
+    return fail(OTS_ERR_UNSUPPORTED, "texture kernel: %d x %d grid (pitch %zu) exceeds the "
+                "2D linear texture limits (%d x %d, pitch alignment %d)",
+                pl->L.n0, pl->L.n1, pitch, maxw, maxh, align);
+  for (int b = 0; b < 2; ++b) {
+    if (reinterpret_cast<uintptr_t>(pl->state[b][0]) % (uintptr_t)align != 0)
+      return fail(OTS_ERR_UNSUPPORTED, "texture kernel: misaligned state buffer");
+    cudaResourceDesc rd{};
+    rd.resType = cudaResourceTypePitch2D;
+    rd.res.pitch2D.devPtr = pl->state[b][0];
+    rd.res.pitch2D.desc = cudaCreateChannelDesc<float>();
+    rd.res.pitch2D.width = (size_t)pl->L.n0;
+    rd.res.pitch2D.height = (size_t)pl->L.n1;
+    rd.res.pitch2D.pitchInBytes = pitch;
+    cudaTextureDesc td{};
+    td.addressMode[0] = cudaAddressModeBorder;
+    td.addressMode[1] = cudaAddressModeBorder;
+    td.filterMode = cudaFilterModePoint;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    OTS_CUDA(cudaCreateTextureObject(&pl->tex[b], &rd, &td, nullptr), "cudaCreateTextureObject");
+  }
+  pl->tex_ok = true;
   return OTS_OK;
 }
 
@@ -513,8 +555,13 @@ void fill_geometry_for_kernel(ots_plan* pl) {
   } else if (g.kernel == OTS_KERNEL_PLAIN) {
     if (pl->K->plain_attr(&a) == cudaSuccess) g.registers = a.numRegs;
   } else {
-    if (pl->K->tile_attr[g.e_axis][pl->prm.elements_per_thread](&a) == cudaSuccess)
+    const int E = pl->prm.elements_per_thread;
+    if (g.kernel == OTS_KERNEL_TEX) {
+      if (E <= ots::kTexMaxE && pl->K->tex_attr[E] && pl->K->tex_attr[E](&a) == cudaSuccess)
+        g.registers = a.numRegs;
+    } else if (pl->K->tile_attr[g.e_axis][E](&a) == cudaSuccess) {
       g.registers = a.numRegs;
+    }
     // resident CTAs per SM from registers, shared memory and threads
     const int thr = g.threads[0] * g.threads[1] * g.threads[2];
     if (a.numRegs > 0 && thr > 0) {
@@ -590,6 +637,15 @@ ots_status enqueue_run(ots_plan* pl, int kernel) {
       }
       e = pl->K->stream[Tl][c.eidx](m, sp, dim3(c.nbx * c.nby, c.nbz * c.cy, 1), dim3(c.bx, c.by, 1),
                                     c.smem, pl->stream);
+      pl->cur ^= 1;
+    }
+  } else if (kernel == OTS_KERNEL_TEX) {
+    const int T = pl->prm.time_tile;
+    auto fn = pl->K->tex[pl->prm.elements_per_thread];
+    for (int base = 0; base < S && e == cudaSuccess; base += T) {
+      ots::StepParams sp = step_params(pl, pl->cur, base, T);
+      sp.tex = pl->tex[pl->cur];
+      e = fn(sp, pl->tile_grid, pl->tile_block, pl->tile_smem, pl->stream);
       pl->cur ^= 1;
     }
   } else {
@@ -678,6 +734,8 @@ void free_plan(ots_plan* pl) {
     if (pl->aux[a]) cudaFree(pl->aux[a]);
   if (pl->d_err) cudaFree(pl->d_err);
   if (pl->d_clocks) cudaFree(pl->d_clocks);
+  for (int b = 0; b < 2; ++b)
+    if (pl->tex[b]) cudaDestroyTextureObject(pl->tex[b]);
   if (pl->ev0) cudaEventDestroy(pl->ev0);
   if (pl->ev1) cudaEventDestroy(pl->ev1);
   if (pl->stream) cudaStreamDestroy(pl->stream);
@@ -849,7 +907,7 @@ static ots_status prepare(const ots_params* params, ots_plan* pl) {
   pl->prm.kernel = k;
   if (k == OTS_KERNEL_STREAM) {
     st = derive_stream(pl, p.time_tile, &pl->scfg);
-  } else if (k == OTS_KERNEL_TILE) {
+  } else if (k == OTS_KERNEL_TILE || k == OTS_KERNEL_TEX) {
     st = validate_tile(pl);
   }
   if (st != OTS_OK) return st;
@@ -907,6 +965,13 @@ ots_status ots_plan_create(const ots_params* params, ots_plan** out) {
     }
     pl->tmap_ok = true;
   }
+  if (k == OTS_KERNEL_TEX) {
+    st = make_textures(pl);
+    if (st != OTS_OK) {
+      free_plan(pl);
+      return st;
+    }
+  }
   *out = pl;
   return OTS_OK;
 }
@@ -961,6 +1026,9 @@ ots_status ots_run_async(ots_plan* plan, int32_t kernel) {
     // a different family than the plan was built for: validate it now
     if (k == OTS_KERNEL_TILE) {
       st = validate_tile(plan);
+    } else if (k == OTS_KERNEL_TEX) {
+      st = validate_tile(plan);
+      if (st == OTS_OK) st = make_textures(plan);
     } else if (k == OTS_KERNEL_STREAM) {
       if (!plan->tmap_ok) {
         st = derive_stream(plan, plan->prm.time_tile, &plan->scfg);
@@ -1168,8 +1236,8 @@ ots_status ots_describe(const ots_plan* plan, ots_kv_fn kv, void* user) {
   emit_i("Padding", g.padding);
   emit_i("Real Size", g.real_size);
   emit_i("Register Usage", g.registers);
-  static const char* kKernel[] = {"auto", "tile", "stream", "plain"};
-  kv("Kernel", kKernel[g.kernel & 3], user);
+  static const char* kKernel[] = {"auto", "tile", "stream", "plain", "tex"};
+  kv("Kernel", kKernel[(g.kernel >= 0 && g.kernel <= 4) ? g.kernel : 0], user);
   emit_i("Dynamic Shared Bytes", g.shared_bytes);
   kv("Engine", p.engine == OTS_ENGINE_COMPAT ? "compat" : "native", user);
   kv("Variant", p.variant == OTS_VARIANT_REF ? "ref" : "baseline", user);

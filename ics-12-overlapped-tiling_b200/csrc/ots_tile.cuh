@@ -47,6 +47,9 @@ struct StepParams {
   // and first step, after the in-tile steps, after the write-back}, indexed
   // by linear block x warps per block; nullptr = off
   unsigned* clocks;
+  // texture path (the reference's jacobi-2d-tex): state field 0 of the input
+  // buffer as a 2D texture with border addressing (0 outside the interior)
+  cudaTextureObject_t tex;
 };
 
 constexpr int kClockWords = 6;
@@ -117,10 +120,12 @@ struct TileThreads {
 
 // Loads for the tile: through the read-only path in the plain tile kernel;
 // at L2 (ld.global.cg) in the batched kernel, whose inputs other CTAs of the
-// same launch have just written.
-template <bool CG>
+// same launch have just written; through the texture unit in the texture
+// variant (state only).
+constexpr int kLoadLdg = 0, kLoadCg = 1, kLoadTex = 2;
+template <int LD>
 __device__ __forceinline__ float tile_load(const float* p) {
-  if constexpr (CG)
+  if constexpr (LD == kLoadCg)
     return __ldcg(p);
   else
     return __ldg(p);
@@ -128,7 +133,7 @@ __device__ __forceinline__ float tile_load(const float* p) {
 
 // One CTA's overlapped time tile.  (bix, biy, biz) is the tile index, (BX,
 // BY, BZ) the logical thread block and (tx, ty, tz) this thread in it.
-template <class Op, int E, int EAX, bool CG>
+template <class Op, int E, int EAX, int LD>
 __device__ __forceinline__ void tile_body(const StepParams& p, int bix, int biy, int biz, int bx,
                                           int by, int bz, int tx, int ty, int tz, float* smem) {
   constexpr int NS = Op::NS, NA = Op::NA;
@@ -166,7 +171,11 @@ __device__ __forceinline__ void tile_body(const StepParams& p, int bix, int biy,
       const int64_t gi = (int64_t)gz * p.L.sz + (int64_t)gy * p.L.sy + gx;
 #pragma unroll
       for (int f = 0; f < NS; ++f) {
-        const float v = in ? tile_load<CG>(p.in[f] + gi) : 0.0f;
+        float v;
+        if constexpr (LD == kLoadTex)  // unnormalised texel centres; border mode gives the ring
+          v = tex2D<float>(p.tex, (float)gx + 0.5f, (float)gy + 0.5f);
+        else
+          v = in ? tile_load<LD>(p.in[f] + gi) : 0.0f;
         cur[f * Lvol + i] = v;
         nxt[f * Lvol + i] = v;  // the ring of the second buffer stays defined
       }
@@ -190,7 +199,8 @@ __device__ __forceinline__ void tile_body(const StepParams& p, int bix, int biy,
     ins[e] = in_domain(p.L, gxs[e], gys[e], gzs[e]);
     const int64_t gi = (int64_t)gzs[e] * p.L.sz + (int64_t)gys[e] * p.L.sy + gxs[e];
 #pragma unroll
-    for (int a = 0; a < NA; ++a) auxv[e][a] = ins[e] ? tile_load<CG>(p.aux[a] + gi) : 0.0f;
+    for (int a = 0; a < NA; ++a)
+      auxv[e][a] = ins[e] ? tile_load<LD == kLoadTex ? kLoadLdg : LD>(p.aux[a] + gi) : 0.0f;
   }
   __syncthreads();
 
@@ -248,8 +258,19 @@ __device__ __forceinline__ void tile_body(const StepParams& p, int bix, int biy,
 template <class Op, int E, int EAX>
 __global__ void __launch_bounds__(TileThreads<E, Op::NS>::kMax) tile_kernel(const StepParams p) {
   extern __shared__ float smem[];
-  tile_body<Op, E, EAX, false>(p, blockIdx.x, blockIdx.y, blockIdx.z, blockDim.x, blockDim.y,
-                               blockDim.z, threadIdx.x, threadIdx.y, threadIdx.z, smem);
+  tile_body<Op, E, EAX, kLoadLdg>(p, blockIdx.x, blockIdx.y, blockIdx.z, blockDim.x, blockDim.y,
+                                  blockDim.z, threadIdx.x, threadIdx.y, threadIdx.z, smem);
+}
+
+// Texture-path variant (opencl/jacobi-2d-tex/jacobi-2d-tex.cpp:235-290): the
+// tile's first-step loads come through the texture unit; the in-tile steps
+// are the same shared-memory steps.  2D, one state field.
+template <class Op, int E>
+__global__ void __launch_bounds__(TileThreads<E, Op::NS>::kMax) tile_tex_kernel(const StepParams p) {
+  static_assert(Op::DIMS == 2 && Op::NS == 1, "texture path: 2D single-field stencils");
+  extern __shared__ float smem[];
+  tile_body<Op, E, 1, kLoadTex>(p, blockIdx.x, blockIdx.y, 0, blockDim.x, blockDim.y, 1,
+                                threadIdx.x, threadIdx.y, 0, smem);
 }
 
 // ------------------------------------------------------------------------

@@ -32,8 +32,8 @@ STENCILS = [
 SID = {n: i for i, n in enumerate(STENCILS)}
 
 ENGINE_NATIVE, ENGINE_COMPAT = 0, 1
-KERNEL_AUTO, KERNEL_TILE, KERNEL_STREAM, KERNEL_PLAIN = 0, 1, 2, 3
-KERNELS = {"auto": 0, "tile": 1, "stream": 2, "plain": 3}
+KERNEL_AUTO, KERNEL_TILE, KERNEL_STREAM, KERNEL_PLAIN, KERNEL_TEX = 0, 1, 2, 3, 4
+KERNELS = {"auto": 0, "tile": 1, "stream": 2, "plain": 3, "tex": 4}
 VARIANT_BASELINE, VARIANT_REF = 0, 1
 
 STATUS = {0: "OK", 1: "INVALID_ARGUMENT", 2: "INVALID_GEOMETRY", 3: "SMEM_TOO_LARGE",

@@ -113,8 +113,8 @@ def stream_space(Ts, bxs, bys, Es, cys=(1,)):
     return out
 
 
-def tile_space(Ts, bxs, bys, bzs, Es):
-    return [dict(kernel="tile", T=T, bx=bx, by=by, bz=bz, E=E)
+def tile_space(Ts, bxs, bys, bzs, Es, kernel="tile"):
+    return [dict(kernel=kernel, T=T, bx=bx, by=by, bz=bz, E=E)
             for T, bx, by, bz, E in itertools.product(Ts, bxs, bys, bzs, Es)]
 
 
@@ -128,7 +128,7 @@ def main(argv=None):
     ap.add_argument("--stencil", required=True, choices=STENCILS)
     ap.add_argument("-n", type=int, required=True)
     ap.add_argument("-t", type=int, default=64)
-    ap.add_argument("--kernel", default="tile", choices=["tile", "stream", "plain"])
+    ap.add_argument("--kernel", default="tile", choices=["tile", "stream", "plain", "tex"])
     ap.add_argument("--engine", default="native", choices=["native", "compat"])
     ap.add_argument("--T", default="1:8:1")
     ap.add_argument("--bx", default="16,32,64")
@@ -145,7 +145,8 @@ def main(argv=None):
     elif a.kernel == "plain":
         space = [dict(kernel="plain", T=1, bx=32, by=8, bz=1, E=1)]
     else:
-        space = tile_space(expand(a.T), expand(a.bx), expand(a.by), expand(a.bz), expand(a.E))
+        space = tile_space(expand(a.T), expand(a.bx), expand(a.by), expand(a.bz), expand(a.E),
+                           kernel=a.kernel)
 
     def log(r):
         if r["status"] == "ok":

@@ -84,12 +84,15 @@ typedef enum ots_engine { OTS_ENGINE_NATIVE = 0, OTS_ENGINE_COMPAT = 1 } ots_eng
 /* Kernel family.  TILE: overlapped time tile in every dimension (the
  * reference scheme).  STREAM: overlapped in x/y, streamed along z with all T
  * time levels in flight (3D star stencils).  PLAIN: one time step per launch
- * (the comparator).  AUTO picks STREAM where available in 3D, else TILE. */
+ * (the comparator).  TEX: the TILE scheme with the first-step loads through
+ * the texture unit (opencl/jacobi-2d-tex/jacobi-2d-tex.cpp; 2D single-field
+ * stencils, E <= 8).  AUTO picks STREAM where available in 3D, else TILE. */
 typedef enum ots_kernel {
   OTS_KERNEL_AUTO = 0,
   OTS_KERNEL_TILE = 1,
   OTS_KERNEL_STREAM = 2,
-  OTS_KERNEL_PLAIN = 3
+  OTS_KERNEL_PLAIN = 3,
+  OTS_KERNEL_TEX = 4
 } ots_kernel;
 
 /* Arithmetic variant where the reference and the benchmark definition

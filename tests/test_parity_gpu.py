@@ -186,6 +186,38 @@ def test_kernel_families_agree_bitwise_on_one_plan():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("st,n,steps,T,bx,by,E", [
+    ("jacobi-2d", 67, 9, 4, 16, 16, 1),
+    ("jacobi-2d", 100, 13, 3, 32, 8, 4),
+    ("jacobi-2d", 33, 5, 2, 16, 4, 8),
+    ("gradient-2d", 70, 7, 3, 16, 8, 2),
+    ("poisson-2d", 71, 8, 3, 32, 8, 2),
+    ("rician-denoise-2d", 66, 6, 2, 16, 8, 1),
+])
+def test_texture_kernel_matches_oracle(st, n, steps, T, bx, by, E):
+    # first-step loads through the texture unit (border addressing = zero ring)
+    g = run_and_check(st, n, steps, T=T, bx=bx, by=by, bz=1, E=E, kernel="tex")
+    assert g.kernel == ots.KERNEL_TEX
+
+
+@pytest.mark.gpu
+def test_texture_kernel_equals_tile_kernel_bitwise_and_rejects_unsupported():
+    with ots.Plan("jacobi-2d", 300, 20, T=4, bx=32, by=8, E=2, kernel="tex") as plan:
+        state, _ = plan.fill_reference(seed=4)
+        outs = []
+        for k in ("tex", "tile", "plain"):
+            plan.upload(state)
+            plan.run(k)
+            outs.append(plan.download()[0])
+    assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
+    assert np.array_equal(outs[0].view(np.uint32), outs[2].view(np.uint32))
+    for kw in (dict(stencil="fdtd-2d", n=64), dict(stencil="jacobi-3d", n=32)):
+        with pytest.raises(ots.OtsError) as ei:
+            ots.Plan(kw["stencil"], kw["n"], 4, T=2, bx=16, by=8, E=1, kernel="tex")
+        assert ei.value.status_name == "UNSUPPORTED"
+
+
+@pytest.mark.gpu
 def test_interior_upload_download_roundtrip():
     with ots.Plan("fdtd-2d", 37, 3, T=2, bx=16, by=8, E=1, kernel="tile") as plan:
         state, _ = plan.fill_reference(seed=8)
