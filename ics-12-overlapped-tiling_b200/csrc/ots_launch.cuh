@@ -14,6 +14,7 @@
 #include <utility>
 
 #include "ots_stream.cuh"
+#include "ots_stream2d.cuh"
 #include "ots_tile.cuh"
 
 namespace ots {
@@ -28,6 +29,8 @@ using TileLaunch = cudaError_t (*)(const StepParams&, dim3, dim3, size_t, cudaSt
 using StreamLaunch = cudaError_t (*)(const CUtensorMap&, const StreamParams&, dim3, dim3, size_t,
                                      cudaStream_t);
 using AttrFn = cudaError_t (*)(cudaFuncAttributes*);
+using Stream2dLaunch = cudaError_t (*)(const Stream2dParams&, dim3, cudaStream_t);
+using Occ2dFn = cudaError_t (*)(int*);
 // stream kernel queries take the cluster flag (the clustered instantiation)
 using StreamAttrFn = cudaError_t (*)(cudaFuncAttributes*, bool);
 using StreamOccFn = cudaError_t (*)(int*, int, size_t, bool);
@@ -43,6 +46,9 @@ struct StencilKernels {
   StreamAttrFn stream_attr[kMaxT + 1][3] = {};
   StreamOccFn stream_occ[kMaxT + 1][3] = {};
   bool has_stream = false;
+  Stream2dLaunch stream2d[kMaxT + 1] = {};  // [T], 2D star stencils
+  AttrFn stream2d_attr[kMaxT + 1] = {};
+  Occ2dFn stream2d_occ[kMaxT + 1] = {};
 };
 
 template <class K>
@@ -149,6 +155,31 @@ void fill_tile(StencilKernels& k, std::integer_sequence<int, Es...>) {
    ...);
 }
 
+template <class Op, int T>
+cudaError_t launch_stream2d(const Stream2dParams& p, dim3 g, cudaStream_t s) {
+  stream2d_kernel<Op, T><<<g, kStream2dThreads, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+template <class Op, int T>
+cudaError_t attr_stream2d(cudaFuncAttributes* a) {
+  return cudaFuncGetAttributes(a, stream2d_kernel<Op, T>);
+}
+
+template <class Op, int T>
+cudaError_t occ_stream2d(int* blocks) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, stream2d_kernel<Op, T>,
+                                                       kStream2dThreads, 0);
+}
+
+template <class Op, int... Ts>
+void fill_stream2d(StencilKernels& k, std::integer_sequence<int, Ts...>) {
+  ((k.stream2d[Ts + 1] = &launch_stream2d<Op, Ts + 1>,
+    k.stream2d_attr[Ts + 1] = &attr_stream2d<Op, Ts + 1>,
+    k.stream2d_occ[Ts + 1] = &occ_stream2d<Op, Ts + 1>),
+   ...);
+}
+
 template <class Op, int... Es>
 void fill_tex(StencilKernels& k, std::integer_sequence<int, Es...>) {
   ((k.tex[Es + 1] = &launch_tex<Op, Es + 1>, k.tex_attr[Es + 1] = &attr_tex<Op, Es + 1>), ...);
@@ -169,6 +200,8 @@ StencilKernels make_kernels() {
   if constexpr (Op::DIMS == 2) fill_tile<Op, 1>(k, std::make_integer_sequence<int, kMaxE>{});
   if constexpr (Op::DIMS == 2 && Op::NS == 1)
     fill_tex<Op>(k, std::make_integer_sequence<int, kTexMaxE>{});
+  if constexpr (Op::DIMS == 2 && HasStar2D<Op>::value)
+    fill_stream2d<Op>(k, std::make_integer_sequence<int, kMaxT>{});
   if constexpr (Op::DIMS == 3) {
     fill_tile<Op, 2>(k, std::make_integer_sequence<int, kMaxE3>{});
     fill_tile<Op, 1>(k, std::make_integer_sequence<int, kMaxE3>{});

@@ -130,6 +130,11 @@ struct OpJacobi2D {
     o[0] = p.coef *
            (a(0, 0, 0, -1) + a(0, 0, 0, 0) + a(0, 0, 0, 1) + a(0, 0, -1, 0) + a(0, 0, 1, 0));
   }
+  // Same arithmetic from the five values (used by the y-streamed kernel).
+  OTS_HD static float star2d(float xm, float c, float xp, float ym, float yp, float,
+                             const OpArgs& p) {
+    return p.coef * (xm + c + xp + ym + yp);
+  }
 };
 
 // Reference: opencl/poisson-2d/poisson-2d.cpp:644-648, 8c - (8 neighbours).
@@ -149,6 +154,12 @@ struct OpPoisson2D {
       o[0] = (s - p.h2 * aux[0]) * 0.25f;
     }
   }
+  // Baseline variant only (the reference variant is 9-point).
+  OTS_HD static float star2d(float xm, float, float xp, float ym, float yp, float f,
+                             const OpArgs& p) {
+    float s = ym + xm + xp + yp;
+    return (s - p.h2 * f) * 0.25f;
+  }
 };
 
 // opencl/gradient-2d/gradient-2d.cpp:283-289: c + rsqrt(1e-4 + sum (c-n)^2)
@@ -161,6 +172,10 @@ struct OpGradient2D {
     float c = a(0, 0, 0, 0);
     o[0] = c + ots_rsqrt(0.0001f + sq(c - a(0, 0, 0, -1)) + sq(c - a(0, 0, 0, 1)) +
                       sq(c - a(0, 0, -1, 0)) + sq(c - a(0, 0, 1, 0)));
+  }
+  OTS_HD static float star2d(float xm, float c, float xp, float ym, float yp, float,
+                             const OpArgs&) {
+    return c + ots_rsqrt(0.0001f + sq(c - xm) + sq(c - xp) + sq(c - ym) + sq(c - yp));
   }
 };
 

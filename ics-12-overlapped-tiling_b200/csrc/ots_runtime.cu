@@ -163,6 +163,12 @@ EncodeTiledFn encode_tiled() {
   return fn;
 }
 
+// y-streamed 2D kernel: 128-cell strips x y segments, one warp each
+struct Stream2dCfg {
+  int T = 0, hx = 0, rpbx = 0, ntx = 0, nseg = 0, zseg = 0, grid = 0;
+  int warps_per_sm = 0;
+};
+
 struct StreamCfg {
   int T = 0, E = 0, eidx = 0, bx = 0, by = 0;
   int cy = 1;              // CTAs per cluster along y (their tiles stack into one)
@@ -202,6 +208,7 @@ struct ots_plan {
   cudaTextureObject_t tex[2] = {0, 0};  // texture kernel: field 0 of state buffer 0 / 1
   bool tex_ok = false;
   StreamCfg scfg;
+  Stream2dCfg s2cfg;
   // tile kernel launch shape
   dim3 tile_grid, tile_block;
   size_t tile_smem = 0;
@@ -328,6 +335,46 @@ ots_status derive(const ots_params* p, ots_geometry* g, const StencilInfo** info
 
 // Stream-kernel shape: bx threads x 4 cells along x, by threads x E rows
 // along y; z split into segments so the CTA count fills whole waves.
+// Strips of 128 cells along x (x halo T rounded up to 4 per side), rows split
+// into segments (block_y > 1: that many rows per segment).  Warps are independent, so the segment count trades the
+// 2T-row pipeline fill of each segment against keeping enough warps per SM
+// to saturate issue: cost = max(warp-iterations / (SMs x saturating warps),
+// one warp's iterations).
+ots_status derive_stream2d(const ots_plan* pl, int T, Stream2dCfg* c) {
+  if (T < 1 || T > ots::kMaxT || !pl->K || !pl->K->stream2d[T])
+    return fail(OTS_ERR_UNSUPPORTED, "2D stream kernel supports T in 1..%d (got %d)",
+                ots::kMaxT, T);
+  c->T = T;
+  c->hx = ots::stream2d_halo(T);
+  c->rpbx = ots::kStream2dWidth - 2 * c->hx;
+  const int n = pl->geo.real_size;
+  c->ntx = ceil_div(n, c->rpbx);
+  int blocks = 0;
+  if (!pl->K->stream2d_occ[T] || pl->K->stream2d_occ[T](&blocks) != cudaSuccess || blocks < 1)
+    blocks = 1;
+  c->warps_per_sm = blocks * (ots::kStream2dThreads / 32);
+  const double sat = (double)std::max(1, pl->sm_count) * std::min(c->warps_per_sm, 12);
+  double best = 1e300;
+  int best_seg = n;
+  for (int nseg = 1; nseg <= std::max(1, n / std::max(1, T)); ++nseg) {
+    const int zseg = ceil_div(n, nseg);
+    const int segs = ceil_div(n, zseg);
+    const double len = zseg + 2.0 * T;
+    const double cost = std::max((double)c->ntx * segs * len / sat, len);
+    if (cost < best * 0.999) {
+      best = cost;
+      best_seg = zseg;
+    }
+  }
+  c->zseg = best_seg;
+  // block_y > 1 sets the rows per segment directly (tuning); else the model
+  if (pl->prm.block_y > 1) c->zseg = std::min(n, pl->prm.block_y);
+  c->nseg = ceil_div(n, c->zseg);
+  const int64_t warps = (int64_t)c->ntx * c->nseg;
+  c->grid = (int)((warps + ots::kStream2dThreads / 32 - 1) / (ots::kStream2dThreads / 32));
+  return OTS_OK;
+}
+
 ots_status derive_stream(const ots_plan* pl, int T, StreamCfg* c) {
   const ots_params& p = pl->prm;
   int eidx = -1;
@@ -431,12 +478,16 @@ ots_status resolve_kernel(ots_plan* pl, int requested, int* out) {
   const StencilInfo& si = *pl->info;
   const bool star_ok = si.star && si.dims == 3 &&
                        !(p.stencil == OTS_POISSON_3D && p.variant == OTS_VARIANT_REF);
+  const bool star2d_ok = si.dims == 2 && pl->K && pl->K->stream2d[1] &&
+                         !(p.stencil == OTS_POISSON_2D && p.variant == OTS_VARIANT_REF);
   int k = requested == OTS_KERNEL_AUTO ? p.kernel : requested;
   if (k == OTS_KERNEL_AUTO)
     k = (star_ok && p.block_z == 1 && p.engine == OTS_ENGINE_NATIVE) ? OTS_KERNEL_STREAM
                                                                       : OTS_KERNEL_TILE;
-  if (k == OTS_KERNEL_STREAM && !star_ok)
-    return fail(OTS_ERR_UNSUPPORTED, "stream kernel covers the 3D star stencils only");
+  if (k == OTS_KERNEL_STREAM && !star_ok && !star2d_ok)
+    return fail(OTS_ERR_UNSUPPORTED,
+                "stream kernel covers the star stencils (jacobi-2d/3d, poisson-2d/3d in the "
+                "baseline variant, gradient-2d/3d)");
   if (k == OTS_KERNEL_TEX &&
       (si.dims != 2 || si.ns != 1 || p.elements_per_thread < 1 ||
        p.elements_per_thread > ots::kTexMaxE || !pl->K->tex[p.elements_per_thread]))
@@ -525,7 +576,31 @@ void fill_geometry_for_kernel(ots_plan* pl) {
   g.kernel = pl->prm.kernel;
   g.sm_count = pl->sm_count;
   cudaFuncAttributes a{};
-  if (g.kernel == OTS_KERNEL_STREAM) {
+  if (g.kernel == OTS_KERNEL_STREAM && g.dims == 2) {
+    const Stream2dCfg& c = pl->s2cfg;
+    g.comps[0] = ots::kStream2dWidth;
+    g.comps[1] = c.zseg + 2 * c.T;
+    g.comps[2] = 1;
+    g.real_per_block[0] = c.rpbx;
+    g.real_per_block[1] = c.zseg;
+    g.real_per_block[2] = 1;
+    g.num_blocks[0] = c.ntx;
+    g.num_blocks[1] = c.nseg;
+    g.num_blocks[2] = 1;
+    g.threads[0] = 32;  // one warp per strip segment
+    g.threads[1] = 1;
+    g.threads[2] = 1;
+    g.e_axis = 0;
+    g.shared_bytes = 0;
+    {
+      const double n = pl->geo.real_size;
+      g.useful_ratio = (n * n) / ((double)ots::kStream2dWidth * c.ntx * c.nseg *
+                                  (double)(c.zseg + 2 * c.T));
+    }
+    if (pl->K->stream2d_attr[c.T] && pl->K->stream2d_attr[c.T](&a) == cudaSuccess)
+      g.registers = a.numRegs;
+    g.ctas_per_sm = c.warps_per_sm / (ots::kStream2dThreads / 32);
+  } else if (g.kernel == OTS_KERNEL_STREAM) {
     const StreamCfg& c = pl->scfg;
     g.comps[0] = c.tx;
     g.comps[1] = c.cy * c.ty;  // a cluster's CTAs share one tile
@@ -603,6 +678,28 @@ ots_status enqueue_run(ots_plan* pl, int kernel) {
     for (int s = 0; s < S && e == cudaSuccess; ++s) {
       ots::StepParams sp = step_params(pl, pl->cur, s, 1);
       e = pl->K->plain(sp, g, b, 0, pl->stream);
+      pl->cur ^= 1;
+    }
+  } else if (kernel == OTS_KERNEL_STREAM && pl->geo.dims == 2) {
+    const int T = pl->prm.time_tile;
+    for (int base = 0; base < S && e == cudaSuccess; base += T) {
+      const int Tl = std::min(T, S - base);
+      Stream2dCfg c = pl->s2cfg;
+      if (Tl != c.T) {
+        ots_status st = derive_stream2d(pl, Tl, &c);
+        if (st != OTS_OK) return st;
+      }
+      ots::Stream2dParams sp{};
+      sp.in = pl->state[pl->cur][0];
+      sp.out = pl->state[pl->cur ^ 1][0];
+      sp.aux = pl->info->na ? pl->aux[0] : nullptr;
+      sp.L = pl->L;
+      sp.ntx = c.ntx;
+      sp.nseg = c.nseg;
+      sp.zseg = c.zseg;
+      sp.base_step = base;
+      sp.op = pl->op;
+      e = pl->K->stream2d[Tl](sp, dim3(c.grid), pl->stream);
       pl->cur ^= 1;
     }
   } else if (kernel == OTS_KERNEL_STREAM) {
@@ -905,7 +1002,9 @@ static ots_status prepare(const ots_params* params, ots_plan* pl) {
   st = resolve_kernel(pl, OTS_KERNEL_AUTO, &k);
   if (st != OTS_OK) return st;
   pl->prm.kernel = k;
-  if (k == OTS_KERNEL_STREAM) {
+  if (k == OTS_KERNEL_STREAM && pl->geo.dims == 2) {
+    st = derive_stream2d(pl, p.time_tile, &pl->s2cfg);
+  } else if (k == OTS_KERNEL_STREAM) {
     st = derive_stream(pl, p.time_tile, &pl->scfg);
   } else if (k == OTS_KERNEL_TILE || k == OTS_KERNEL_TEX) {
     st = validate_tile(pl);
@@ -956,7 +1055,7 @@ ots_status ots_plan_create(const ots_params* params, ots_plan** out) {
     free_plan(pl);
     return s2;
   }
-  if (k == OTS_KERNEL_STREAM) {
+  if (k == OTS_KERNEL_STREAM && pl->geo.dims == 3) {
     st = make_tmap(pl, pl->scfg, pl->state[0][0], &pl->tmap[0]);
     if (st == OTS_OK) st = make_tmap(pl, pl->scfg, pl->state[1][0], &pl->tmap[1]);
     if (st != OTS_OK) {
@@ -1029,6 +1128,8 @@ ots_status ots_run_async(ots_plan* plan, int32_t kernel) {
     } else if (k == OTS_KERNEL_TEX) {
       st = validate_tile(plan);
       if (st == OTS_OK) st = make_textures(plan);
+    } else if (k == OTS_KERNEL_STREAM && plan->geo.dims == 2) {
+      if (plan->s2cfg.T == 0) st = derive_stream2d(plan, plan->prm.time_tile, &plan->s2cfg);
     } else if (k == OTS_KERNEL_STREAM) {
       if (!plan->tmap_ok) {
         st = derive_stream(plan, plan->prm.time_tile, &plan->scfg);

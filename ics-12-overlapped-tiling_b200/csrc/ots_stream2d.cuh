@@ -1,0 +1,176 @@
+// ots_stream2d.cuh -- y-streamed overlapped time tile for 2D star stencils.
+//
+// The 2D counterpart of the z-streamed kernel: one warp owns an x strip of
+// 128 cells (4 consecutive cells per lane) and walks a y segment row by row
+// with all T time levels in flight; level t works on row k - t while row k
+// arrives.  x is overlapped (a halo of T cells per side, rounded up to 4 so
+// every row access is a 16-byte vector), y needs no redundant halo (only the
+// 2T-1 rows of pipeline fill per segment).  Each level keeps its three newest
+// rows of own cells in registers; x neighbours travel by warp shuffle (lane
+// 0's left and lane 31's right are strip-edge halo cells whose values are
+// never used).  There is no shared memory and no block-wide barrier: warps
+// are independent, and input rows are fetched from global memory (L2 for
+// grids that fit it) three rows ahead of use.
+//
+// Operand order per update is the stencil's own (Op::star2d), so results are
+// bit-identical to the tile and plain kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <type_traits>
+
+#include "ots_tile.cuh"
+
+namespace ots {
+
+struct Stream2dParams {
+  const float* in;
+  float* out;
+  const float* aux;  // Poisson f, or nullptr
+  Layout L;          // n0 = x extent, n1 = y extent, sy = row pitch
+  int ntx;           // x strips
+  int nseg;          // y segments
+  int zseg;          // rows per segment
+  int base_step;
+  OpArgs op;
+};
+
+// Stencils with the five-point form star2d(x-1, c, x+1, y-1, y+1, f).
+template <class Op, class = void>
+struct HasStar2D : std::false_type {};
+template <class Op>
+struct HasStar2D<Op, std::void_t<decltype(&Op::star2d)>> : std::true_type {};
+
+constexpr int kStream2dThreads = 128;  // 4 independent warps per CTA
+constexpr int kStream2dWidth = 128;    // cells per strip (32 lanes x 4)
+
+__host__ __device__ inline int stream2d_halo(int T) { return (T + 3) / 4 * 4; }
+
+template <int N>
+struct Phase2 {
+  static constexpr int value = N;
+};
+
+template <class Op, int T>
+__global__ void __launch_bounds__(kStream2dThreads)
+    stream2d_kernel(const __grid_constant__ Stream2dParams p) {
+  constexpr int V = 4;
+  constexpr int HX = (T + 3) / 4 * 4;
+  constexpr int RPBX = kStream2dWidth - 2 * HX;
+  const int lane = threadIdx.x & 31;
+  const int w = blockIdx.x * (kStream2dThreads / 32) + (threadIdx.x >> 5);
+  if (w >= p.ntx * p.nseg) return;  // whole warps only
+  const int strip = w % p.ntx, seg = w / p.ntx;
+  const int nx = p.L.n0, ny = p.L.n1;
+  const int64_t sy = p.L.sy;
+  const int tx0 = strip * RPBX - HX;  // multiple of 4
+  const int lx = V * lane;
+  const int gx = tx0 + lx;
+  unsigned xin = 0;
+#pragma unroll
+  for (int v = 0; v < V; ++v)
+    if ((unsigned)(gx + v) < (unsigned)nx) xin |= 1u << v;
+  const bool xall = xin == 0xFu;
+  const bool wx = lx >= HX && lx < HX + RPBX;  // this lane's cells are output columns
+  const int ys = seg * p.zseg;
+  const int ye = min(ny, ys + p.zseg);
+  const int kb = ys - T;
+  const int nit = (ye + T - 1) - kb + 1;
+
+  // one input row (zeros outside the domain)
+  auto load_row = [&](int k, float (&d)[V]) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) d[v] = 0.0f;
+    if ((unsigned)k < (unsigned)ny) {
+      const float* src = p.in + (int64_t)k * sy + gx;
+      if (xall) {
+        const float4 a = __ldg(reinterpret_cast<const float4*>(src));
+        d[0] = a.x; d[1] = a.y; d[2] = a.z; d[3] = a.w;
+      } else {
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+          if ((xin >> v) & 1) d[v] = __ldg(src + v);
+      }
+    }
+  };
+
+  float R[T][3][V];  // level t (0 = input): three newest rows of own cells
+#pragma unroll
+  for (int t = 0; t < T; ++t)
+#pragma unroll
+    for (int s = 0; s < 3; ++s)
+#pragma unroll
+      for (int v = 0; v < V; ++v) R[t][s][v] = 0.0f;
+  float P[3][V];  // prefetched input rows k .. k+2
+#pragma unroll
+  for (int j = 0; j < 3; ++j) load_row(kb + j, P[j]);
+
+  auto step = [&](auto ph, int r) {
+    constexpr int PH = decltype(ph)::value;
+    constexpr int SN = PH, SC = (PH + 2) % 3, SM = (PH + 1) % 3;  // newest, centre, y-1
+    const int k = kb + r;
+    // level 0: the prefetched row k; its slot takes row k + 3
+#pragma unroll
+    for (int v = 0; v < V; ++v) R[0][SN][v] = P[PH][v];
+    load_row(k + 3, P[PH]);
+#pragma unroll
+    for (int t = 1; t <= T; ++t) {
+      const int q = k - t;
+      const float(&C)[V] = R[t - 1][SC];
+      const float(&M)[V] = R[t - 1][SM];
+      const float(&N)[V] = R[t - 1][SN];
+      const float lv = __shfl_up_sync(0xffffffffu, C[V - 1], 1);
+      const float rv = __shfl_down_sync(0xffffffffu, C[0], 1);
+      const bool qin = (unsigned)q < (unsigned)ny;
+      float f[V] = {0.0f, 0.0f, 0.0f, 0.0f};
+      if (Op::NA > 0 && qin) {
+        const float* src = p.aux + (int64_t)q * sy + gx;
+        if (xall) {
+          const float4 a = __ldg(reinterpret_cast<const float4*>(src));
+          f[0] = a.x; f[1] = a.y; f[2] = a.z; f[3] = a.w;
+        } else {
+#pragma unroll
+          for (int v = 0; v < V; ++v)
+            if ((xin >> v) & 1) f[v] = __ldg(src + v);
+        }
+      }
+      // level T writes the slot of level T-1's oldest row, which no level
+      // needs any more; each cell reads M[v] before its own out[v] is written
+      float(&out)[V] = (t < T) ? R[t < T ? t : 0][SN] : R[T - 1][SM];
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const float xm = v > 0 ? C[v - 1] : lv;
+        const float xp = v < V - 1 ? C[v + 1] : rv;
+        out[v] = Op::star2d(xm, C[v], xp, M[v], N[v], f[v], p.op);
+      }
+      if (!(qin && xall)) {  // domain edge: the Dirichlet ring stays zero
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+          if (!(qin && ((xin >> v) & 1))) out[v] = 0.0f;
+      }
+      if (t == T && q >= ys && q < ye && wx) {
+        float* dst = p.out + (int64_t)q * sy + gx;
+        if (xall) {
+          *reinterpret_cast<float4*>(dst) = make_float4(out[0], out[1], out[2], out[3]);
+        } else {
+#pragma unroll
+          for (int v = 0; v < V; ++v)
+            if ((xin >> v) & 1) dst[v] = out[v];
+        }
+      }
+    }
+  };
+
+  int r = 0;
+  for (; r + 2 < nit; r += 3) {
+    step(Phase2<0>{}, r);
+    step(Phase2<1>{}, r + 1);
+    step(Phase2<2>{}, r + 2);
+  }
+  if (r < nit) step(Phase2<0>{}, r++);
+  if (r < nit) step(Phase2<1>{}, r++);
+}
+
+}  // namespace ots

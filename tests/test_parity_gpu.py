@@ -218,6 +218,50 @@ def test_texture_kernel_equals_tile_kernel_bitwise_and_rejects_unsupported():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("st", ["jacobi-2d", "poisson-2d", "gradient-2d"])
+@pytest.mark.parametrize("T", [1, 2, 3, 4, 5, 8])
+def test_stream2d_kernel_matches_oracle(st, T):
+    # y-streamed 2D kernel: n not a multiple of the strip interior, several
+    # y segments, the last launch shallower than T
+    g = run_and_check(st, 301, 2 * T + 1, T=T, bx=32, by=1, E=1, kernel="stream")
+    assert g.kernel == ots.KERNEL_STREAM and g.num_blocks[0] >= 3
+
+
+@pytest.mark.gpu
+def test_stream2d_small_and_edge_grids():
+    for n, steps, T in ((5, 3, 2), (128, 9, 4), (129, 7, 8), (1000, 13, 6)):
+        run_and_check("jacobi-2d", n, steps, T=T, bx=32, by=1, E=1, kernel="stream")
+    for steps in (0, 1):
+        run_and_check("jacobi-2d", 64, steps, T=4, bx=32, by=1, E=1, kernel="stream")
+    with pytest.raises(ots.OtsError) as ei:
+        ots.Plan("poisson-2d", 64, 4, T=2, bx=32, by=1, E=1, kernel="stream",
+                 variant=ots.VARIANT_REF)
+    assert ei.value.status_name == "UNSUPPORTED"
+
+
+@pytest.mark.gpu
+def test_stream2d_full_size_equals_tile_and_plain_bitwise():
+    """jacobi-2d 2048^2 x 64 steps (the 2D workload): stream, tile and plain
+    kernels give identical bits."""
+    with ots.Plan("jacobi-2d", 2048, 64, T=8, bx=32, by=1, E=1, kernel="stream") as plan:
+        state, _ = plan.fill_reference(seed=123456)
+        g = plan.geometry
+        inner = np.ascontiguousarray(state[0][g.padding:g.padding + 2048,
+                                              g.padding:g.padding + 2048])
+        outs = []
+        for k in ("stream", "plain"):
+            plan.upload_interior([inner])
+            plan.run(k)
+            outs.append(plan.download_interior()[0])
+    with ots.Plan("jacobi-2d", 2048, 64, T=4, bx=16, by=16, E=1, kernel="tile") as plan:
+        plan.upload_interior([inner])
+        plan.run()
+        outs.append(plan.download_interior()[0])
+    assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
+    assert np.array_equal(outs[0].view(np.uint32), outs[2].view(np.uint32))
+
+
+@pytest.mark.gpu
 def test_interior_upload_download_roundtrip():
     with ots.Plan("fdtd-2d", 37, 3, T=2, bx=16, by=8, E=1, kernel="tile") as plan:
         state, _ = plan.fill_reference(seed=8)
