@@ -56,6 +56,38 @@ int orc_set_threads(int n) {
   return g_orc_threads;
 }
 
+/* Whole-array copies (the reference's per-step memcpy) split over the same
+ * threads: a byte copy, so the result does not depend on the split. */
+typedef struct {
+  char* d;
+  const char* s;
+  size_t n;
+} orc_copy_job;
+
+static void* orc_copy_thread(void* p) {
+  orc_copy_job* j = (orc_copy_job*)p;
+  memcpy(j->d, j->s, j->n);
+  return 0;
+}
+
+static void orc_par_copy(void* dst, const void* src, size_t bytes, int nth) {
+  if (nth <= 1 || bytes < ((size_t)1 << 22)) {
+    memcpy(dst, src, bytes);
+    return;
+  }
+  if (nth > ORC_MAX_THREADS) nth = ORC_MAX_THREADS;
+  pthread_t th[ORC_MAX_THREADS];
+  orc_copy_job jobs[ORC_MAX_THREADS];
+  for (int k = 0; k < nth; ++k) {
+    const size_t a = bytes * (size_t)k / (size_t)nth, b = bytes * (size_t)(k + 1) / (size_t)nth;
+    jobs[k].d = (char*)dst + a;
+    jobs[k].s = (const char*)src + a;
+    jobs[k].n = b - a;
+    pthread_create(&th[k], 0, orc_copy_thread, &jobs[k]);
+  }
+  for (int k = 0; k < nth; ++k) pthread_join(th[k], 0);
+}
+
 /* ------------------------------------------------------------------ */
 /* Stencil constants (reference file:line cited at each use).          */
 /* ------------------------------------------------------------------ */
