@@ -142,13 +142,20 @@ def dist_setup():
 
 
 def reduce_max(t, world):
+    """Max over ranks (the slowest replica sets the job's time)."""
     if world == 1:
         return t
     import torch
     import torch.distributed as dist
-    x = torch.tensor([t], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    x = torch.tensor([t], dtype=torch.float64, device=dev)
     dist.all_reduce(x, op=dist.ReduceOp.MAX)
     return float(x.item())
+
+
+def job_value(updates_per_rank, world, seconds_max):
+    """Whole-job GUpdates/s: every rank's updates over the slowest rank's time."""
+    return float(updates_per_rank) * world / seconds_max / 1e9
 
 
 def barrier(world):
@@ -268,7 +275,7 @@ def main():
         el = timed(cfg["kernel"], args.steps)
     el_max = reduce_max(el, world)
     updates = float(N) ** 3 * STEPS * args.steps * world
-    value = updates / el_max / 1e9
+    value = job_value(float(N) ** 3 * STEPS * args.steps, world, el_max)
     avg_launch = el / (args.steps * launches_per_step)
 
     # plain one-step comparator (same plan, same data)
