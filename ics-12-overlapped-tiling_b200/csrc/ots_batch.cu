@@ -18,6 +18,13 @@
 //   * per grid, the tile shape (T, block x, E) is its own -- chosen by the
 //     cost model -- from the menu instantiated here;
 //   * the counter reset and the launch are captured once in a CUDA graph.
+//
+// Stream mode (every grid's kernel = OTS_KERNEL_STREAM): the items are one
+// warp's strip x y-segment of the y-streamed 2D kernel (stream2d_body) for
+// one time chunk; each warp takes its own item and waits (bounded) for the
+// grid's previous chunk, with the same queue order and counters.  T <= 4 keeps
+// the strip halo (and so the strips) the same for a grid's last, shallower
+// chunk.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -34,11 +41,14 @@ void ots_set_last_error(const char* msg);
 namespace ots {
 
 constexpr int kBatchThreads = 256;
+constexpr int kBatchStreamThreads = 128;
+constexpr int kBatchStreamMaxT = 4;
 
 struct BatchGrid {
   int op;             // 0 jacobi-2d, 1 poisson-2d, 2 gradient-2d
   int n, steps, T, bx, eidx;
-  int ntx, nty, rpbx, rpby;
+  int ntx, nty, rpbx, rpby;  // stream mode: nty = y segments
+  int zseg;                  // stream mode: rows per segment
   int chunks;
   int cnt_off;        // this grid's first chunk counter
   int64_t sy;
@@ -132,6 +142,80 @@ __global__ void __launch_bounds__(kBatchThreads) batch_kernel(const BatchGrid* _
   }
 }
 
+template <class Op>
+__device__ __forceinline__ void batch_stream_unit(const Stream2dParams& p, int T, int strip,
+                                                  int seg) {
+  switch (T) {
+    case 1: stream2d_body<Op, 1, kLoadCg>(p, strip, seg); break;
+    case 2: stream2d_body<Op, 2, kLoadCg>(p, strip, seg); break;
+    case 3: stream2d_body<Op, 3, kLoadCg>(p, strip, seg); break;
+    default: stream2d_body<Op, 4, kLoadCg>(p, strip, seg); break;
+  }
+}
+
+__global__ void __launch_bounds__(kBatchStreamThreads)
+    batch_stream_kernel(const BatchGrid* __restrict__ grids, const int4* __restrict__ items,
+                        int nitems, int* next, int* counters, int* err) {
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    int it = 0;
+    if (lane == 0) it = atomicAdd(next, 1);
+    it = __shfl_sync(0xffffffffu, it, 0);
+    if (it >= nitems) break;
+    const int4 w = items[it];
+    const BatchGrid& g = grids[w.x];
+    int ok = 1;
+    if (lane == 0) {
+      ok = *(volatile int*)err == 0;
+      if (ok && w.y > 0) {
+        const int need = g.ntx * g.nty;
+        volatile int* c = counters + g.cnt_off + w.y - 1;
+        const uint64_t t0 = batch_ns();
+        unsigned i = 0;
+        while (*c < need) {
+          if (*(volatile int*)err != 0) {
+            ok = 0;
+            break;
+          }
+          if ((++i & 63) == 0 && batch_ns() - t0 > 2000000000ull) {
+            atomicOr(err, 2);
+            ok = 0;
+            break;
+          }
+          __nanosleep(64);
+        }
+      }
+    }
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    if (!ok) break;
+    __threadfence();  // acquire: the previous chunk's writes are visible to every lane
+    Stream2dParams p{};
+    p.in = g.buf[w.y & 1];
+    p.out = g.buf[(w.y + 1) & 1];
+    p.aux = g.aux;
+    p.L.n0 = g.n;
+    p.L.n1 = g.n;
+    p.L.n2 = 1;
+    p.L.sy = g.sy;
+    p.L.sz = g.sy * g.n;
+    p.ntx = g.ntx;
+    p.nseg = g.nty;
+    p.zseg = g.zseg;
+    p.base_step = w.y * g.T;
+    p.op = g.op_args;
+    const int Tl = min(g.T, g.steps - w.y * g.T);  // the last chunk may be shallower
+    const int seg = w.z / g.ntx, strip = w.z - seg * g.ntx;
+    switch (g.op) {
+      case 0: batch_stream_unit<OpJacobi2D>(p, Tl, strip, seg); break;
+      case 1: batch_stream_unit<OpPoisson2D>(p, Tl, strip, seg); break;
+      default: batch_stream_unit<OpGradient2D>(p, Tl, strip, seg); break;
+    }
+    __threadfence();  // release: this lane's writes before the count
+    __syncwarp();
+    if (lane == 0) atomicAdd(counters + g.cnt_off + w.y, 1);
+  }
+}
+
 }  // namespace ots
 
 struct ots_batch {
@@ -148,6 +232,7 @@ struct ots_batch {
   size_t smem = 0;
   int ctas = 0;
   int64_t updates = 0;
+  bool stream_mode = false;  // items are warps of the y-streamed 2D kernel
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaGraph_t graph = nullptr;
@@ -194,8 +279,14 @@ ots_status enqueue_batch(ots_batch* b) {
   const int nc = b->ncounters;
   B_CUDA(cudaMemsetAsync(b->d_counters, 0, (size_t)(nc + 2) * sizeof(int), b->stream),
          "reset counters");
-  ots::batch_kernel<<<b->ctas, ots::kBatchThreads, b->smem, b->stream>>>(
-      b->d_grids, b->d_items, b->nitems, b->d_counters + nc, b->d_counters, b->d_counters + nc + 1);
+  if (b->stream_mode)
+    ots::batch_stream_kernel<<<b->ctas, ots::kBatchStreamThreads, 0, b->stream>>>(
+        b->d_grids, b->d_items, b->nitems, b->d_counters + nc, b->d_counters,
+        b->d_counters + nc + 1);
+  else
+    ots::batch_kernel<<<b->ctas, ots::kBatchThreads, b->smem, b->stream>>>(
+        b->d_grids, b->d_items, b->nitems, b->d_counters + nc, b->d_counters,
+        b->d_counters + nc + 1);
   B_CUDA(cudaGetLastError(), "batch kernel launch");
   return OTS_OK;
 }
@@ -222,9 +313,15 @@ ots_status ots_batch_create(const ots_params* grids, int32_t n, int32_t device, 
   size_t floats = 0;
   std::vector<size_t> off(n);
   int cnt = 0;
+  b->stream_mode = grids[0].kernel == OTS_KERNEL_STREAM;
   for (int i = 0; i < n; ++i) {
     const ots_params& p = grids[i];
     ots::BatchGrid g{};
+    if ((p.kernel == OTS_KERNEL_STREAM) != b->stream_mode) {
+      free_batch(b);
+      return bfail(OTS_ERR_UNSUPPORTED,
+                   "batched grids must all use the stream kernel or all the tile kernel");
+    }
     switch (p.stencil) {
       case OTS_JACOBI_2D: g.op = 0; break;
       case OTS_POISSON_2D: g.op = 1; break;
@@ -237,29 +334,49 @@ ots_status ots_batch_create(const ots_params* grids, int32_t n, int32_t device, 
       free_batch(b);
       return bfail(OTS_ERR_INVALID_ARGUMENT, "batched grid: need n >= 1, steps >= 0, 1 <= T <= 8");
     }
-    if (!(p.block_x == 16 || p.block_x == 32 || p.block_x == 64)) {
-      free_batch(b);
-      return bfail(OTS_ERR_UNSUPPORTED, "batched grid: block x must be 16, 32 or 64 (256 threads)");
-    }
-    const int E = p.elements_per_thread;
-    g.eidx = E == 1 ? 0 : E == 2 ? 1 : E == 4 ? 2 : -1;
-    if (g.eidx < 0) {
-      free_batch(b);
-      return bfail(OTS_ERR_UNSUPPORTED, "batched grid: E must be 1, 2 or 4");
-    }
     g.n = p.problem_size;
     g.steps = p.time_steps;
     g.T = p.time_tile;
-    g.bx = p.block_x;
-    const int by = ots::kBatchThreads / g.bx;
-    g.rpbx = g.bx - 2 * (g.T - 1);
-    g.rpby = by * E - 2 * (g.T - 1);
-    if (g.rpbx < 1 || g.rpby < 1) {
-      free_batch(b);
-      return bfail(OTS_ERR_INVALID_GEOMETRY, "batched grid: T too deep for its block");
+    if (b->stream_mode) {
+      if (g.T > ots::kBatchStreamMaxT) {
+        free_batch(b);
+        return bfail(OTS_ERR_UNSUPPORTED, "batched stream grid: T must be 1..4");
+      }
+      if (g.op == 1 && p.variant == OTS_VARIANT_REF) {
+        free_batch(b);
+        return bfail(OTS_ERR_UNSUPPORTED, "batched stream grid: poisson-2d baseline variant only");
+      }
+      // strips of 128 cells with a 4-cell halo (T <= 4); block_y > 1 = rows per segment
+      g.rpbx = ots::kStream2dWidth - 2 * ots::stream2d_halo(ots::kBatchStreamMaxT);
+      g.zseg = std::min(g.n, p.block_y > 1 ? p.block_y : 64);
+      g.rpby = g.zseg;
+      g.ntx = (g.n + g.rpbx - 1) / g.rpbx;
+      g.nty = (g.n + g.zseg - 1) / g.zseg;
+      g.bx = 32;
+      g.eidx = 0;
+    } else {
+      if (!(p.block_x == 16 || p.block_x == 32 || p.block_x == 64)) {
+        free_batch(b);
+        return bfail(OTS_ERR_UNSUPPORTED,
+                     "batched grid: block x must be 16, 32 or 64 (256 threads)");
+      }
+      const int E = p.elements_per_thread;
+      g.eidx = E == 1 ? 0 : E == 2 ? 1 : E == 4 ? 2 : -1;
+      if (g.eidx < 0) {
+        free_batch(b);
+        return bfail(OTS_ERR_UNSUPPORTED, "batched grid: E must be 1, 2 or 4");
+      }
+      g.bx = p.block_x;
+      const int by = ots::kBatchThreads / g.bx;
+      g.rpbx = g.bx - 2 * (g.T - 1);
+      g.rpby = by * E - 2 * (g.T - 1);
+      if (g.rpbx < 1 || g.rpby < 1) {
+        free_batch(b);
+        return bfail(OTS_ERR_INVALID_GEOMETRY, "batched grid: T too deep for its block");
+      }
+      g.ntx = (g.n + g.rpbx - 1) / g.rpbx;
+      g.nty = (g.n + g.rpby - 1) / g.rpby;
     }
-    g.ntx = (g.n + g.rpbx - 1) / g.rpbx;
-    g.nty = (g.n + g.rpby - 1) / g.rpby;
     g.chunks = g.steps > 0 ? (g.steps + g.T - 1) / g.T : 0;
     g.cnt_off = cnt;
     cnt += std::max(1, g.chunks);
@@ -303,16 +420,26 @@ ots_status ots_batch_create(const ots_params* grids, int32_t n, int32_t device, 
   b->nitems = (int)items.size();
   // shared bytes: the largest tile of the menu (block 256 threads, E <= 4)
   size_t smem = 0;
-  for (auto& g : b->grids) {
-    const int by = ots::kBatchThreads / g.bx;
-    const int E = g.eidx == 0 ? 1 : g.eidx == 1 ? 2 : 4;
-    smem = std::max(smem, (size_t)2 * (g.bx + 2) * (by * E + 2) * sizeof(float));
-  }
+  if (!b->stream_mode)
+    for (auto& g : b->grids) {
+      const int by = ots::kBatchThreads / g.bx;
+      const int E = g.eidx == 0 ? 1 : g.eidx == 1 ? 2 : 4;
+      smem = std::max(smem, (size_t)2 * (g.bx + 2) * (by * E + 2) * sizeof(float));
+    }
   b->smem = smem;
   int per_sm = 1, sms = 1;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ots::batch_kernel, ots::kBatchThreads, smem);
-  b->ctas = std::max(1, std::min(sms * std::max(1, per_sm), std::max(1, b->nitems)));
+  if (b->stream_mode) {
+    // persistent warps: every resident slot, at most one warp per item
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ots::batch_stream_kernel,
+                                                  ots::kBatchStreamThreads, 0);
+    const int wpc = ots::kBatchStreamThreads / 32;
+    b->ctas = std::max(1, std::min(sms * std::max(1, per_sm), (std::max(1, b->nitems) + wpc - 1) / wpc));
+  } else {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ots::batch_kernel, ots::kBatchThreads,
+                                                  smem);
+    b->ctas = std::max(1, std::min(sms * std::max(1, per_sm), std::max(1, b->nitems)));
+  }
   e = cudaMalloc(&b->d_grids, n * sizeof(ots::BatchGrid));
   if (e == cudaSuccess) e = cudaMemcpy(b->d_grids, b->grids.data(), n * sizeof(ots::BatchGrid), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMalloc(&b->d_items, std::max<size_t>(1, items.size()) * sizeof(int4));
@@ -435,8 +562,11 @@ ots_status ots_batch_run_async(ots_batch* b) {
 // with the grid's own (T, block, E).
 ots_status ots_batch_run_sequential(ots_batch* b, int32_t kernel, ots_timing* timing) {
   if (!b) return bfail(OTS_ERR_INVALID_ARGUMENT, "batch is NULL");
-  if (kernel != OTS_KERNEL_PLAIN && kernel != OTS_KERNEL_TILE)
-    return bfail(OTS_ERR_INVALID_ARGUMENT, "sequential kernel must be PLAIN or TILE");
+  if (kernel != OTS_KERNEL_PLAIN && kernel != OTS_KERNEL_TILE && kernel != OTS_KERNEL_STREAM)
+    return bfail(OTS_ERR_INVALID_ARGUMENT, "sequential kernel must be PLAIN, TILE or STREAM");
+  if ((kernel == OTS_KERNEL_STREAM) != b->stream_mode && kernel != OTS_KERNEL_PLAIN)
+    return bfail(OTS_ERR_INVALID_ARGUMENT,
+                 "sequential TILE / STREAM must match the batch's kernel family");
   B_CUDA(cudaSetDevice(b->device), "cudaSetDevice");
   static const int kStencil[3] = {OTS_JACOBI_2D, OTS_POISSON_2D, OTS_GRADIENT_2D};
   int launches = 0;
@@ -463,6 +593,32 @@ ots_status ots_batch_run_sequential(ots_batch* b, int32_t kernel, ots_timing* ti
         sp.out[0] = g.buf[cur ^ 1];
         sp.base_step = t;
         B_CUDA(K.plain(sp, grd, blk, 0, b->stream), "plain launch");
+        cur ^= 1;
+        ++launches;
+      }
+    } else if (kernel == OTS_KERNEL_STREAM) {
+      // the same strips, one y-streamed launch per chunk, with the segment
+      // length a grid run on its own gets (more, shorter segments than in
+      // the batch, where the other grids fill the GPU)
+      int blocks = 1, sms = 148;
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+      if (!K.stream2d_occ[g.T] || K.stream2d_occ[g.T](&blocks) != cudaSuccess || blocks < 1)
+        blocks = 1;
+      ots::Stream2dParams s2{};
+      s2.aux = g.aux;
+      s2.L = sp.L;
+      s2.ntx = g.ntx;
+      s2.zseg = ots::stream2d_zseg(g.n, g.T, g.ntx, sms, blocks * (ots::kStream2dThreads / 32));
+      s2.nseg = (g.n + s2.zseg - 1) / s2.zseg;
+      s2.op = g.op_args;
+      const int wpc = ots::kStream2dThreads / 32;
+      const dim3 grd((g.ntx * s2.nseg + wpc - 1) / wpc);
+      for (int c = 0; c < g.chunks; ++c) {
+        const int Tl = std::min(g.T, g.steps - c * g.T);
+        s2.in = g.buf[cur];
+        s2.out = g.buf[cur ^ 1];
+        s2.base_step = c * g.T;
+        B_CUDA(K.stream2d[Tl](s2, grd, b->stream), "stream launch");
         cur ^= 1;
         ++launches;
       }

@@ -333,13 +333,9 @@ ots_status derive(const ots_params* p, ots_geometry* g, const StencilInfo** info
   return OTS_OK;
 }
 
-// Stream-kernel shape: bx threads x 4 cells along x, by threads x E rows
-// along y; z split into segments so the CTA count fills whole waves.
-// Strips of 128 cells along x (x halo T rounded up to 4 per side), rows split
-// into segments (block_y > 1: that many rows per segment).  Warps are independent, so the segment count trades the
-// 2T-row pipeline fill of each segment against keeping enough warps per SM
-// to saturate issue: cost = max(warp-iterations / (SMs x saturating warps),
-// one warp's iterations).
+// 2D stream kernel: strips of 128 cells along x (x halo T rounded up to 4 per side), rows split
+// into segments (block_y > 1: that many rows per segment; else
+// stream2d_zseg's choice).
 ots_status derive_stream2d(const ots_plan* pl, int T, Stream2dCfg* c) {
   if (T < 1 || T > ots::kMaxT || !pl->K || !pl->K->stream2d[T])
     return fail(OTS_ERR_UNSUPPORTED, "2D stream kernel supports T in 1..%d (got %d)",
@@ -353,20 +349,7 @@ ots_status derive_stream2d(const ots_plan* pl, int T, Stream2dCfg* c) {
   if (!pl->K->stream2d_occ[T] || pl->K->stream2d_occ[T](&blocks) != cudaSuccess || blocks < 1)
     blocks = 1;
   c->warps_per_sm = blocks * (ots::kStream2dThreads / 32);
-  const double sat = (double)std::max(1, pl->sm_count) * std::min(c->warps_per_sm, 12);
-  double best = 1e300;
-  int best_seg = n;
-  for (int nseg = 1; nseg <= std::max(1, n / std::max(1, T)); ++nseg) {
-    const int zseg = ceil_div(n, nseg);
-    const int segs = ceil_div(n, zseg);
-    const double len = zseg + 2.0 * T;
-    const double cost = std::max((double)c->ntx * segs * len / sat, len);
-    if (cost < best * 0.999) {
-      best = cost;
-      best_seg = zseg;
-    }
-  }
-  c->zseg = best_seg;
+  c->zseg = ots::stream2d_zseg(n, T, c->ntx, pl->sm_count, c->warps_per_sm);
   // block_y > 1 sets the rows per segment directly (tuning); else the model
   if (pl->prm.block_y > 1) c->zseg = std::min(n, pl->prm.block_y);
   c->nseg = ceil_div(n, c->zseg);
@@ -375,6 +358,8 @@ ots_status derive_stream2d(const ots_plan* pl, int T, Stream2dCfg* c) {
   return OTS_OK;
 }
 
+// Stream-kernel shape: bx threads x 4 cells along x, by threads x E rows
+// along y; z split into segments so the CTA count fills whole waves.
 ots_status derive_stream(const ots_plan* pl, int T, StreamCfg* c) {
   const ots_params& p = pl->prm;
   int eidx = -1;

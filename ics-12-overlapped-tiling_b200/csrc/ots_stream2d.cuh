@@ -48,21 +48,59 @@ constexpr int kStream2dWidth = 128;    // cells per strip (32 lanes x 4)
 
 __host__ __device__ inline int stream2d_halo(int T) { return (T + 3) / 4 * 4; }
 
+// Rows per y segment for one grid on its own.  Warps are independent, so the
+// segment count trades the 2T-row pipeline fill of each segment against
+// keeping enough warps per SM to saturate issue: cost = max(warp-iterations /
+// (SMs x saturating warps), one warp's iterations).
+inline int stream2d_zseg(int n, int T, int ntx, int sm_count, int warps_per_sm) {
+  const double sat = (double)(sm_count > 1 ? sm_count : 1) * (warps_per_sm < 12 ? warps_per_sm : 12);
+  double best = 1e300;
+  int best_seg = n;
+  const int maxseg = n / (T > 1 ? T : 1) > 1 ? n / (T > 1 ? T : 1) : 1;
+  for (int nseg = 1; nseg <= maxseg; ++nseg) {
+    const int zseg = (n + nseg - 1) / nseg;
+    const int segs = (n + zseg - 1) / zseg;
+    const double len = zseg + 2.0 * T;
+    const double work = (double)ntx * segs * len / (sat > 0 ? sat : 1.0);
+    const double cost = work > len ? work : len;
+    if (cost < best * 0.999) {
+      best = cost;
+      best_seg = zseg;
+    }
+  }
+  return best_seg;
+}
+
 template <int N>
 struct Phase2 {
   static constexpr int value = N;
 };
 
-template <class Op, int T>
-__global__ void __launch_bounds__(kStream2dThreads)
-    stream2d_kernel(const __grid_constant__ Stream2dParams p) {
+// Row loads: through the read-only path (standalone kernel) or at L2 (the
+// batched kernel, whose inputs other SMs have just written).
+template <int LD>
+__device__ __forceinline__ float4 s2_load4(const float* p) {
+  if constexpr (LD == kLoadCg)
+    return __ldcg(reinterpret_cast<const float4*>(p));
+  else
+    return __ldg(reinterpret_cast<const float4*>(p));
+}
+template <int LD>
+__device__ __forceinline__ float s2_load1(const float* p) {
+  if constexpr (LD == kLoadCg)
+    return __ldcg(p);
+  else
+    return __ldg(p);
+}
+
+// One warp's strip x segment: the whole time tile of T levels.  Called by
+// all 32 lanes of a warp together (shuffles).
+template <class Op, int T, int LD>
+__device__ __forceinline__ void stream2d_body(const Stream2dParams& p, int strip, int seg) {
   constexpr int V = 4;
   constexpr int HX = (T + 3) / 4 * 4;
   constexpr int RPBX = kStream2dWidth - 2 * HX;
   const int lane = threadIdx.x & 31;
-  const int w = blockIdx.x * (kStream2dThreads / 32) + (threadIdx.x >> 5);
-  if (w >= p.ntx * p.nseg) return;  // whole warps only
-  const int strip = w % p.ntx, seg = w / p.ntx;
   const int nx = p.L.n0, ny = p.L.n1;
   const int64_t sy = p.L.sy;
   const int tx0 = strip * RPBX - HX;  // multiple of 4
@@ -86,12 +124,12 @@ __global__ void __launch_bounds__(kStream2dThreads)
     if ((unsigned)k < (unsigned)ny) {
       const float* src = p.in + (int64_t)k * sy + gx;
       if (xall) {
-        const float4 a = __ldg(reinterpret_cast<const float4*>(src));
+        const float4 a = s2_load4<LD>(src);
         d[0] = a.x; d[1] = a.y; d[2] = a.z; d[3] = a.w;
       } else {
 #pragma unroll
         for (int v = 0; v < V; ++v)
-          if ((xin >> v) & 1) d[v] = __ldg(src + v);
+          if ((xin >> v) & 1) d[v] = s2_load1<LD>(src + v);
       }
     }
   };
@@ -128,12 +166,12 @@ __global__ void __launch_bounds__(kStream2dThreads)
       if (Op::NA > 0 && qin) {
         const float* src = p.aux + (int64_t)q * sy + gx;
         if (xall) {
-          const float4 a = __ldg(reinterpret_cast<const float4*>(src));
+          const float4 a = s2_load4<kLoadLdg>(src);  // read-only for the whole run
           f[0] = a.x; f[1] = a.y; f[2] = a.z; f[3] = a.w;
         } else {
 #pragma unroll
           for (int v = 0; v < V; ++v)
-            if ((xin >> v) & 1) f[v] = __ldg(src + v);
+            if ((xin >> v) & 1) f[v] = s2_load1<kLoadLdg>(src + v);
         }
       }
       // level T writes the slot of level T-1's oldest row, which no level
@@ -171,6 +209,14 @@ __global__ void __launch_bounds__(kStream2dThreads)
   }
   if (r < nit) step(Phase2<0>{}, r++);
   if (r < nit) step(Phase2<1>{}, r++);
+}
+
+template <class Op, int T>
+__global__ void __launch_bounds__(kStream2dThreads)
+    stream2d_kernel(const __grid_constant__ Stream2dParams p) {
+  const int w = blockIdx.x * (kStream2dThreads / 32) + (threadIdx.x >> 5);
+  if (w >= p.ntx * p.nseg) return;  // whole warps only
+  stream2d_body<Op, T, kLoadLdg>(p, w % p.ntx, w / p.ntx);
 }
 
 }  // namespace ots

@@ -4,10 +4,12 @@
 
 runs the batched workload -- 256 independent FP32 grids mixing jacobi-2d,
 poisson-2d (Jacobi sweep with RHS) and gradient-2d, sides log-uniform in
-[64, 2048], step counts uniform in 8..256, inputs uniform [0, 1) -- with each
-grid's (T, block, E) picked by the learned cost model, and prints one JSON
-line: aggregate GUpdates/s of the single graph launch against the same grids
-run one after another (one launch per step, and one tile launch per T steps).
+[64, 2048], step counts uniform in 8..256, inputs uniform [0, 1) -- in two
+single graph launches: tile items with each grid's (T, block, E) picked by the
+learned cost model, and warp items of the y-streamed 2D kernel (T = 4, or the
+grid's step count if smaller); it prints one JSON line with their aggregate
+GUpdates/s against the same grids run one after another (one launch per step,
+one tile launch per T steps, one streamed launch per T steps).
 """
 import argparse
 import ctypes
@@ -17,8 +19,8 @@ import os
 
 import numpy as np
 
-from . import (KERNEL_PLAIN, KERNEL_TILE, OtsError, Params, SID, Timing, check, derive_geometry,
-               lib, make_params)
+from . import (KERNEL_PLAIN, KERNEL_STREAM, KERNEL_TILE, OtsError, Params, SID, Timing, check,
+               derive_geometry, lib, make_params)
 
 BATCH_STENCILS = ("jacobi-2d", "poisson-2d", "gradient-2d")
 MENU = [dict(T=T, bx=bx, E=E) for T in range(1, 9) for bx in (16, 32, 64) for E in (1, 2, 4)]
@@ -90,12 +92,27 @@ def pick(grids, cost_model=None, device=0):
     return grids
 
 
+def pick_stream(grids, T=4, rows=1):
+    """Stream-mode choice per grid: T (at most 4, at most the step count) and
+    rows per segment (1 = the library's default)."""
+    for g in grids:
+        g.update(kernel="stream", T=max(1, min(T, g["steps"])), bx=32, by=rows, E=1)
+    return grids
+
+
 class Batch:
+    """Grids with kernel="stream" (all of them) run as warp items of the
+    y-streamed 2D kernel; otherwise as tile items with their own (T, bx, E)."""
+
     def __init__(self, grids, device=0):
         arr = (Params * len(grids))()
         for i, g in enumerate(grids):
-            arr[i] = make_params(g["stencil"], g["n"], g["steps"], T=g["T"], bx=g["bx"],
-                                 by=256 // g["bx"], E=g["E"], device=device)
+            if g.get("kernel") == "stream":
+                arr[i] = make_params(g["stencil"], g["n"], g["steps"], T=g["T"], bx=32,
+                                     by=g.get("by", 1), E=1, kernel="stream", device=device)
+            else:
+                arr[i] = make_params(g["stencil"], g["n"], g["steps"], T=g["T"], bx=g["bx"],
+                                     by=256 // g["bx"], E=g["E"], device=device)
         h = ctypes.c_void_p()
         check(_blib().ots_batch_create(arr, len(grids), device, ctypes.byref(h)))
         self.h = h
@@ -139,7 +156,7 @@ class Batch:
 
     def run_sequential(self, kernel="plain"):
         t = Timing()
-        k = KERNEL_PLAIN if kernel == "plain" else KERNEL_TILE
+        k = {"plain": KERNEL_PLAIN, "tile": KERNEL_TILE, "stream": KERNEL_STREAM}[kernel]
         check(_blib().ots_batch_run_sequential(self.h, k, ctypes.byref(t)))
         return t.event_ms * 1e-3, t.launches
 
@@ -194,6 +211,31 @@ def main(argv=None):
     upd = info["updates"]
     tg = sorted(t_graph)[len(t_graph) // 2]
     tt = sorted(t_tile)[len(t_tile) // 2]
+    b.close()
+    # the same grids as warp items of the y-streamed kernel
+    sgrids = pick_stream([dict(g) for g in grids])
+    bs = Batch(sgrids)
+
+    def load_s():
+        for i, (s, x) in enumerate(ins):
+            bs.upload(i, s, x)
+
+    load_s()
+    bs.run()
+    t_sg = []
+    for _ in range(a.reps):
+        load_s()
+        t_sg.append(bs.run())
+    load_s()
+    bs.run_sequential("stream")
+    t_ss = []
+    for _ in range(max(1, a.reps // 2)):
+        load_s()
+        t_ss.append(bs.run_sequential("stream")[0])
+    sinfo = bs.info()
+    bs.close()
+    tsg = sorted(t_sg)[len(t_sg) // 2]
+    tss = sorted(t_ss)[len(t_ss) // 2]
     print(json.dumps({
         "metric": "GUpdates/s", "workload": "batched: %d grids jacobi-2d/poisson-2d/gradient-2d, "
         "sides 64..2048 log-uniform, steps 8..256 (seed %d)" % (a.grids, a.seed),
@@ -204,8 +246,11 @@ def main(argv=None):
                              "launches": launches},
         "speedup_vs_sequential_plain": t_plain / tg, "speedup_vs_sequential_tile": tt / tg,
         "configs_from": "cost model" if cm is not None else "default T=4 32x8 E=2",
+        "stream_graph_one_launch": {"value": upd / tsg / 1e9, "seconds": tsg,
+                                    "items": sinfo["items"], "ctas": sinfo["ctas"]},
+        "sequential_stream": {"value": upd / tss / 1e9, "seconds": tss},
+        "stream_speedup_vs_sequential_plain": t_plain / tsg,
     }))
-    b.close()
     return 0
 
 

@@ -28,6 +28,10 @@ def space(stencil, dims, quick=False):
     elif dims == 2:
         for T, bx, by, E in itertools.product(range(1, 9), (16, 32, 64), (4, 8, 16), (1, 2, 4, 8)):
             cfgs.append(dict(kernel="tile", T=T, bx=bx, by=by, bz=1, E=E))
+        if stencil in ("jacobi-2d", "poisson-2d", "gradient-2d"):
+            # y-streamed kernel: T and rows per segment (by; 1 = the library's choice)
+            for T, by in itertools.product(range(1, 9), (1, 16, 32, 64, 128)):
+                cfgs.append(dict(kernel="stream", T=T, bx=32, by=by, bz=1, E=1))
     else:
         for T, (bx, by, bz), E in itertools.product(
                 range(1, 5), ((32, 4, 4), (32, 8, 2), (64, 4, 2), (16, 8, 4), (16, 16, 2)),
@@ -45,7 +49,7 @@ def geom_dict(g):
     return {k: (list(v) if hasattr(v, "__len__") else v) for k, v in g.as_dict().items()}
 
 
-def collect(stencils=None, quick=False, reps=3, device=0, log=print):
+def collect(stencils=None, quick=False, reps=3, device=0, log=print, kernel=None):
     records = []
     for st in stencils or STENCILS:
         dims = {"jacobi-1d": 1, "jacobi-1d-5pt": 1, "jacobi-1d-7pt": 1}.get(
@@ -55,6 +59,8 @@ def collect(stencils=None, quick=False, reps=3, device=0, log=print):
         t0 = time.time()
         ok = 0
         for cfg in space(st, dims, quick):
+            if kernel and cfg["kernel"] != kernel:
+                continue
             rec = dict(stencil=st, n=n, steps=steps, **cfg)
             try:
                 plan = Plan(st, n, steps, device=device, **cfg)
@@ -90,8 +96,15 @@ def main(argv=None):
     ap.add_argument("--stencils", default=",".join(STENCILS))
     ap.add_argument("--quick", action="store_true")
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--kernel", help="collect only this kernel family's configurations")
+    ap.add_argument("--merge", help="existing dataset: keep its records of other "
+                    "(stencil, kernel) pairs and replace the collected ones")
     a = ap.parse_args(argv)
-    recs = collect(a.stencils.split(","), a.quick, a.reps)
+    recs = collect(a.stencils.split(","), a.quick, a.reps, kernel=a.kernel)
+    if a.merge:
+        old = json.load(open(a.merge))["records"]
+        got = {(r["stencil"], r["kernel"]) for r in recs}
+        recs = [r for r in old if (r["stencil"], r["kernel"]) not in got] + recs
     with open(a.out, "w") as fh:
         json.dump({"device": "B200", "workload": {str(k): v for k, v in WORKLOAD.items()},
                    "records": recs}, fh, separators=(",", ":"))

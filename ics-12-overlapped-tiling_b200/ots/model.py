@@ -261,6 +261,17 @@ def leave_one_out(records, k_frac=0.10, hidden=64, layers=3, epochs=300, batch=1
         spearman = float(np.corrcoef(rp, ra)[0, 1]) if len(te) > 2 else 0.0
         best_rec = rows[te[int(np.argmax(actual))]]
         pick_rec = rows[te[int(top[int(np.argmax(actual[top]))])]]
+        # the same model ranking the tile-kernel configurations alone (the space
+        # the reference's analytical model can rank)
+        tile_only = None
+        tsel = np.array([i for i, j in enumerate(te) if rows[j].get("kernel", "tile") == "tile"])
+        if len(tsel) >= 2:
+            at, pt = actual[tsel], np.asarray(pred)[tsel]
+            kt = max(1, int(math.floor(k_frac * len(tsel))))
+            order = np.argsort(-pt)
+            tile_only = {"space": int(len(tsel)), "k": kt,
+                         "picked_over_best": float(np.max(at[order[:kt]]) / np.max(at)),
+                         "top1_over_best": float(at[order[0]] / np.max(at))}
         report[s] = {
             "space": len(te), "k": k, "measure_cost": k / float(len(te)),
             "best_gupdates": best, "picked_gupdates": picked, "picked_over_best": picked / best,
@@ -269,6 +280,7 @@ def leave_one_out(records, k_frac=0.10, hidden=64, layers=3, epochs=300, batch=1
             "train_loss": loss,
             "best_config": {q: best_rec[q] for q in ("kernel", "T", "bx", "by", "bz", "E")},
             "picked_config": {q: pick_rec[q] for q in ("kernel", "T", "bx", "by", "bz", "E")},
+            "tile_only": tile_only,
         }
         m.close()
     if report:
