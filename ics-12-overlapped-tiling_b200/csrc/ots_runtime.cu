@@ -770,6 +770,15 @@ ots_status copy_field(ots_plan* pl, float* dev, const float* host, bool to_dev, 
                          : (size_t)pad + (d >= 2 ? (size_t)pad * P : 0) +
                                (d == 3 ? (size_t)pad * P * P : 0);
   const cudaMemcpyKind kind = to_dev ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
+  // dense host array and unpadded device rows: one linear copy
+  if (interior_only_host && L.sy == L.n0) {
+    const size_t bytes = (size_t)L.n0 * L.n1 * L.n2 * sizeof(float);
+    if (to_dev)
+      OTS_CUDA(cudaMemcpyAsync(dev, host, bytes, kind, pl->stream), "upload");
+    else
+      OTS_CUDA(cudaMemcpyAsync((float*)host, dev, bytes, kind, pl->stream), "download");
+    return OTS_OK;
+  }
   if (d == 1) {
     if (to_dev)
       OTS_CUDA(cudaMemcpyAsync(dev, host + off, L.n0 * sizeof(float), kind, pl->stream), "upload");
@@ -1069,17 +1078,20 @@ ots_status ots_plan_geometry(const ots_plan* plan, ots_geometry* out) {
 }
 
 static ots_status upload_impl(ots_plan* pl, const float* const* state, const float* const* aux,
-                              bool interior) {
+                              bool interior, bool wait = true) {
   if (!pl || !state) return fail(OTS_ERR_INVALID_ARGUMENT, "NULL argument");
   OTS_CUDA(cudaSetDevice(pl->device), "cudaSetDevice");
   for (int f = 0; f < pl->info->ns; ++f) {
     if (!state[f]) return fail(OTS_ERR_INVALID_ARGUMENT, "state field %d is NULL", f);
-    // both ping-pong buffers get the input, as the reference writes it twice
-    for (int b = 0; b < 2; ++b) {
-      ots_status s = copy_field(pl, pl->state[b][f], state[f], true, pl->geo.padding,
-                                pl->geo.padded_size, interior);
-      if (s != OTS_OK) return s;
-    }
+    // both ping-pong buffers get the input, as the reference writes it twice:
+    // once from the host, then on the device
+    ots_status s = copy_field(pl, pl->state[0][f], state[f], true, pl->geo.padding,
+                              pl->geo.padded_size, interior);
+    if (s != OTS_OK) return s;
+    OTS_CUDA(cudaMemcpyAsync(pl->state[1][f], pl->state[0][f],
+                             (size_t)pl->field_elems * sizeof(float), cudaMemcpyDeviceToDevice,
+                             pl->stream),
+             "device copy");
   }
   for (int a = 0; a < pl->info->na; ++a) {
     if (!aux || !aux[a]) return fail(OTS_ERR_INVALID_ARGUMENT, "aux field %d is NULL", a);
@@ -1088,7 +1100,7 @@ static ots_status upload_impl(ots_plan* pl, const float* const* state, const flo
     if (s != OTS_OK) return s;
   }
   pl->cur = 0;
-  OTS_CUDA(cudaStreamSynchronize(pl->stream), "upload");
+  if (wait) OTS_CUDA(cudaStreamSynchronize(pl->stream), "upload");
   return OTS_OK;
 }
 
@@ -1098,6 +1110,15 @@ ots_status ots_upload(ots_plan* plan, const float* const* state, const float* co
 
 ots_status ots_upload_interior(ots_plan* plan, const float* const* state, const float* const* aux) {
   return upload_impl(plan, state, aux, true);
+}
+
+ots_status ots_upload_async(ots_plan* plan, const float* const* state, const float* const* aux) {
+  return upload_impl(plan, state, aux, false, false);
+}
+
+ots_status ots_upload_interior_async(ots_plan* plan, const float* const* state,
+                                     const float* const* aux) {
+  return upload_impl(plan, state, aux, true, false);
 }
 
 ots_status ots_run_async(ots_plan* plan, int32_t kernel) {
@@ -1161,7 +1182,8 @@ ots_status ots_run(ots_plan* plan, int32_t kernel, ots_timing* timing) {
   return OTS_OK;
 }
 
-static ots_status download_impl(ots_plan* pl, float* const* state, bool interior) {
+static ots_status download_impl(ots_plan* pl, float* const* state, bool interior,
+                                bool wait = true) {
   if (!pl || !state) return fail(OTS_ERR_INVALID_ARGUMENT, "NULL argument");
   OTS_CUDA(cudaSetDevice(pl->device), "cudaSetDevice");
   for (int f = 0; f < pl->info->ns; ++f) {
@@ -1170,8 +1192,16 @@ static ots_status download_impl(ots_plan* pl, float* const* state, bool interior
                               pl->geo.padded_size, interior);
     if (s != OTS_OK) return s;
   }
-  OTS_CUDA(cudaStreamSynchronize(pl->stream), "download");
+  if (wait) OTS_CUDA(cudaStreamSynchronize(pl->stream), "download");
   return OTS_OK;
+}
+
+ots_status ots_download_async(ots_plan* plan, float* const* state) {
+  return download_impl(plan, state, false, false);
+}
+
+ots_status ots_download_interior_async(ots_plan* plan, float* const* state) {
+  return download_impl(plan, state, true, false);
 }
 
 ots_status ots_download(ots_plan* plan, float* const* state) {

@@ -127,10 +127,12 @@ def lib():
     L.ots_plan_geometry.restype = st
     L.ots_derive_geometry.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(Geometry)]
     L.ots_derive_geometry.restype = st
-    for fn in ("ots_upload", "ots_upload_interior"):
+    for fn in ("ots_upload", "ots_upload_interior", "ots_upload_async",
+               "ots_upload_interior_async"):
         getattr(L, fn).argtypes = [ctypes.c_void_p, ctypes.POINTER(_FP), ctypes.POINTER(_FP)]
         getattr(L, fn).restype = st
-    for fn in ("ots_download", "ots_download_interior"):
+    for fn in ("ots_download", "ots_download_interior", "ots_download_async",
+               "ots_download_interior_async"):
         getattr(L, fn).argtypes = [ctypes.c_void_p, ctypes.POINTER(_FP)]
         getattr(L, fn).restype = st
     L.ots_run.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(Timing)]
@@ -293,6 +295,27 @@ class Plan:
         st = self._checked(state, g.num_fields, self.interior_shape, "state")
         ax = self._checked(aux, g.num_aux, self.interior_shape, "aux")
         check(lib().ots_upload_interior(self.handle, _fptrs(st), _fptrs(ax) if ax else None))
+
+    def upload_interior_async(self, state, aux=()):
+        """Enqueue the upload and return; the arrays (C-contiguous float32,
+        ideally page-locked) must stay alive and unchanged until sync()."""
+        g = self.geometry
+        st = self._checked(state, g.num_fields, self.interior_shape, "state")
+        ax = self._checked(aux, g.num_aux, self.interior_shape, "aux")
+        if any(a is not b for a, b in zip(st, state)) or any(a is not b for a, b in zip(ax, aux)):
+            raise ValueError("upload_interior_async: arrays must already be C-contiguous float32")
+        check(lib().ots_upload_interior_async(self.handle, _fptrs(st), _fptrs(ax) if ax else None))
+
+    def download_interior_async(self, out):
+        """Enqueue the copy of the current state into `out` and return; valid
+        after sync()."""
+        g = self.geometry
+        for a in out:
+            if a.shape != self.interior_shape or a.dtype != np.float32 or not a.flags.c_contiguous:
+                raise ValueError("download: need C-contiguous float32 %s" % (self.interior_shape,))
+        if len(out) != g.num_fields:
+            raise ValueError("download: expected %d arrays" % g.num_fields)
+        check(lib().ots_download_interior_async(self.handle, _fptrs(out)))
 
     def run(self, kernel=KERNEL_AUTO):
         t = Timing()

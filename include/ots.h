@@ -237,6 +237,19 @@ ots_status ots_sync(ots_plan* plan);
 ots_status ots_download(ots_plan* plan, float* const* state);
 ots_status ots_download_interior(ots_plan* plan, float* const* state);
 
+/* The four copies above, enqueued on the plan's stream without waiting
+ * (the reference's non-blocking enqueueWriteBuffer/enqueueReadBuffer,
+ * jacobi-2d.cpp:874-886, 952-954, with blocking off).  Host arrays must stay
+ * valid and unchanged until ots_sync returns; with page-locked host memory
+ * (ots_host_register) the copies overlap other plans' kernels, so several
+ * plans on one GPU can pipeline upload, run and download of independent
+ * problems. */
+ots_status ots_upload_async(ots_plan* plan, const float* const* state, const float* const* aux);
+ots_status ots_upload_interior_async(ots_plan* plan, const float* const* state,
+                                     const float* const* aux);
+ots_status ots_download_async(ots_plan* plan, float* const* state);
+ots_status ots_download_interior_async(ots_plan* plan, float* const* state);
+
 /* Report the reference runner's key/value lines (printProgramParameters and
  * the per-stencil model constants, jacobi-2d.cpp:1029-1037) through `kv`. */
 typedef void (*ots_kv_fn)(const char* key, const char* value, void* user);

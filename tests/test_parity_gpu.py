@@ -262,6 +262,34 @@ def test_stream2d_full_size_equals_tile_and_plain_bitwise():
 
 
 @pytest.mark.gpu
+def test_async_copies_pipeline_two_plans_like_the_blocking_calls():
+    kw = dict(T=3, bx=16, by=8, bz=1, E=2, kernel="stream")
+    with ots.Plan("poisson-3d", 70, 7, **kw) as a, ots.Plan("poisson-3d", 70, 7, **kw) as b:
+        inner = [np.random.default_rng(s).random((70, 70, 70), dtype=np.float32) for s in (1, 2)]
+        f = np.random.default_rng(3).random((70, 70, 70), dtype=np.float32)
+        a.upload_interior([inner[0]], [f])
+        a.run()
+        want0 = a.download_interior()[0]
+        a.upload_interior([inner[1]], [f])
+        a.run()
+        want1 = a.download_interior()[0]
+        outs = [[np.zeros_like(inner[0])] for _ in range(4)]
+        for s in range(4):  # a, b, a, b: each plan reused while the other runs
+            pl = (a, b)[s % 2]
+            pl.upload_interior_async([inner[s % 2]], [f])
+            pl.run_async()
+            pl.download_interior_async(outs[s])
+        a.sync()
+        b.sync()
+    for s in range(4):
+        want = want0 if s % 2 == 0 else want1
+        assert np.array_equal(outs[s][0].view(np.uint32), want.view(np.uint32)), s
+    with pytest.raises(ValueError):
+        with ots.Plan("jacobi-3d", 16, 2, **kw) as c:
+            c.upload_interior_async([np.zeros((16, 16, 16), np.float64)])
+
+
+@pytest.mark.gpu
 def test_interior_upload_download_roundtrip():
     with ots.Plan("fdtd-2d", 37, 3, T=2, bx=16, by=8, E=1, kernel="tile") as plan:
         state, _ = plan.fill_reference(seed=8)
