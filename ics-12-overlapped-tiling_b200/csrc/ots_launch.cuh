@@ -30,6 +30,8 @@ using StreamLaunch = cudaError_t (*)(const CUtensorMap&, const StreamParams&, di
                                      cudaStream_t);
 using AttrFn = cudaError_t (*)(cudaFuncAttributes*);
 using Stream2dLaunch = cudaError_t (*)(const Stream2dParams&, dim3, cudaStream_t);
+using Stream2dgLaunch = cudaError_t (*)(const Stream2dgParams&, dim3, cudaStream_t);
+constexpr int kMaxTg = 6;  // generic 2D stream kernel levels
 using Occ2dFn = cudaError_t (*)(int*);
 // stream kernel queries take the cluster flag (the clustered instantiation)
 using StreamAttrFn = cudaError_t (*)(cudaFuncAttributes*, bool);
@@ -49,6 +51,9 @@ struct StencilKernels {
   Stream2dLaunch stream2d[kMaxT + 1] = {};  // [T], 2D star stencils
   AttrFn stream2d_attr[kMaxT + 1] = {};
   Occ2dFn stream2d_occ[kMaxT + 1] = {};
+  Stream2dgLaunch stream2dg[kMaxTg + 1] = {};  // [T], any 2D stencil through apply()
+  AttrFn stream2dg_attr[kMaxTg + 1] = {};
+  Occ2dFn stream2dg_occ[kMaxTg + 1] = {};
 };
 
 template <class K>
@@ -172,6 +177,31 @@ cudaError_t occ_stream2d(int* blocks) {
                                                        kStream2dThreads, 0);
 }
 
+template <class Op, int T>
+cudaError_t launch_stream2dg(const Stream2dgParams& p, dim3 g, cudaStream_t s) {
+  stream2dg_kernel<Op, T><<<g, kStream2dThreads, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+template <class Op, int T>
+cudaError_t attr_stream2dg(cudaFuncAttributes* a) {
+  return cudaFuncGetAttributes(a, stream2dg_kernel<Op, T>);
+}
+
+template <class Op, int T>
+cudaError_t occ_stream2dg(int* blocks) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, stream2dg_kernel<Op, T>,
+                                                       kStream2dThreads, 0);
+}
+
+template <class Op, int... Ts>
+void fill_stream2dg(StencilKernels& k, std::integer_sequence<int, Ts...>) {
+  ((k.stream2dg[Ts + 1] = &launch_stream2dg<Op, Ts + 1>,
+    k.stream2dg_attr[Ts + 1] = &attr_stream2dg<Op, Ts + 1>,
+    k.stream2dg_occ[Ts + 1] = &occ_stream2dg<Op, Ts + 1>),
+   ...);
+}
+
 template <class Op, int... Ts>
 void fill_stream2d(StencilKernels& k, std::integer_sequence<int, Ts...>) {
   ((k.stream2d[Ts + 1] = &launch_stream2d<Op, Ts + 1>,
@@ -202,6 +232,10 @@ StencilKernels make_kernels() {
     fill_tex<Op>(k, std::make_integer_sequence<int, kTexMaxE>{});
   if constexpr (Op::DIMS == 2 && HasStar2D<Op>::value)
     fill_stream2d<Op>(k, std::make_integer_sequence<int, kMaxT>{});
+  // the generic streamed kernel where the five-point form does not cover the
+  // op (several fields, aux fields, or other neighbours)
+  if constexpr (Op::DIMS == 2 && (Op::NS > 1 || Op::NA > 0 || !HasStar2D<Op>::value))
+    fill_stream2dg<Op>(k, std::make_integer_sequence<int, kMaxTg>{});
   if constexpr (Op::DIMS == 3) {
     fill_tile<Op, 2>(k, std::make_integer_sequence<int, kMaxE3>{});
     fill_tile<Op, 1>(k, std::make_integer_sequence<int, kMaxE3>{});

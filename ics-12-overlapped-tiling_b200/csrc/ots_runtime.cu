@@ -167,6 +167,8 @@ EncodeTiledFn encode_tiled() {
 struct Stream2dCfg {
   int T = 0, hx = 0, rpbx = 0, ntx = 0, nseg = 0, zseg = 0, grid = 0;
   int warps_per_sm = 0;
+  bool generic = false;  // stream2dg_kernel (the op's apply through register rows)
+  int R = 1;             // rows of reach per level
 };
 
 struct StreamCfg {
@@ -336,20 +338,29 @@ ots_status derive(const ots_params* p, ots_geometry* g, const StencilInfo** info
 // 2D stream kernel: strips of 128 cells along x (x halo T rounded up to 4 per side), rows split
 // into segments (block_y > 1: that many rows per segment; else
 // stream2d_zseg's choice).
+bool star2d_usable(const ots_plan* pl) {
+  return pl->K && pl->K->stream2d[1] &&
+         !(pl->prm.stencil == OTS_POISSON_2D && pl->prm.variant == OTS_VARIANT_REF);
+}
+
 ots_status derive_stream2d(const ots_plan* pl, int T, Stream2dCfg* c) {
-  if (T < 1 || T > ots::kMaxT || !pl->K || !pl->K->stream2d[T])
-    return fail(OTS_ERR_UNSUPPORTED, "2D stream kernel supports T in 1..%d (got %d)",
-                ots::kMaxT, T);
+  c->generic = !star2d_usable(pl);
+  c->R = c->generic ? pl->info->ry : 1;
+  const int maxT = c->generic ? ots::kMaxTg : ots::kMaxT;
+  const bool have = T >= 1 && T <= maxT && pl->K &&
+                    (c->generic ? pl->K->stream2dg[T] != nullptr : pl->K->stream2d[T] != nullptr);
+  if (!have)
+    return fail(OTS_ERR_UNSUPPORTED, "2D stream kernel supports T in 1..%d (got %d)", maxT, T);
   c->T = T;
-  c->hx = ots::stream2d_halo(T);
+  c->hx = ots::stream2d_halo(c->R * T);
   c->rpbx = ots::kStream2dWidth - 2 * c->hx;
   const int n = pl->geo.real_size;
   c->ntx = ceil_div(n, c->rpbx);
   int blocks = 0;
-  if (!pl->K->stream2d_occ[T] || pl->K->stream2d_occ[T](&blocks) != cudaSuccess || blocks < 1)
-    blocks = 1;
+  auto occ = c->generic ? pl->K->stream2dg_occ[T] : pl->K->stream2d_occ[T];
+  if (!occ || occ(&blocks) != cudaSuccess || blocks < 1) blocks = 1;
   c->warps_per_sm = blocks * (ots::kStream2dThreads / 32);
-  c->zseg = ots::stream2d_zseg(n, T, c->ntx, pl->sm_count, c->warps_per_sm);
+  c->zseg = ots::stream2d_zseg(n, c->R * T, c->ntx, pl->sm_count, c->warps_per_sm);
   // block_y > 1 sets the rows per segment directly (tuning); else the model
   if (pl->prm.block_y > 1) c->zseg = std::min(n, pl->prm.block_y);
   c->nseg = ceil_div(n, c->zseg);
@@ -463,16 +474,15 @@ ots_status resolve_kernel(ots_plan* pl, int requested, int* out) {
   const StencilInfo& si = *pl->info;
   const bool star_ok = si.star && si.dims == 3 &&
                        !(p.stencil == OTS_POISSON_3D && p.variant == OTS_VARIANT_REF);
-  const bool star2d_ok = si.dims == 2 && pl->K && pl->K->stream2d[1] &&
-                         !(p.stencil == OTS_POISSON_2D && p.variant == OTS_VARIANT_REF);
+  const bool star2d_ok = si.dims == 2 && (star2d_usable(pl) || (pl->K && pl->K->stream2dg[1]));
   int k = requested == OTS_KERNEL_AUTO ? p.kernel : requested;
   if (k == OTS_KERNEL_AUTO)
     k = (star_ok && p.block_z == 1 && p.engine == OTS_ENGINE_NATIVE) ? OTS_KERNEL_STREAM
                                                                       : OTS_KERNEL_TILE;
   if (k == OTS_KERNEL_STREAM && !star_ok && !star2d_ok)
     return fail(OTS_ERR_UNSUPPORTED,
-                "stream kernel covers the star stencils (jacobi-2d/3d, poisson-2d/3d in the "
-                "baseline variant, gradient-2d/3d)");
+                "stream kernel covers the 2D stencils and the 3D star stencils (jacobi-3d, "
+                "poisson-3d in the baseline variant, gradient-3d)");
   if (k == OTS_KERNEL_TEX &&
       (si.dims != 2 || si.ns != 1 || p.elements_per_thread < 1 ||
        p.elements_per_thread > ots::kTexMaxE || !pl->K->tex[p.elements_per_thread]))
@@ -564,7 +574,7 @@ void fill_geometry_for_kernel(ots_plan* pl) {
   if (g.kernel == OTS_KERNEL_STREAM && g.dims == 2) {
     const Stream2dCfg& c = pl->s2cfg;
     g.comps[0] = ots::kStream2dWidth;
-    g.comps[1] = c.zseg + 2 * c.T;
+    g.comps[1] = c.zseg + 2 * c.R * c.T;
     g.comps[2] = 1;
     g.real_per_block[0] = c.rpbx;
     g.real_per_block[1] = c.zseg;
@@ -580,10 +590,10 @@ void fill_geometry_for_kernel(ots_plan* pl) {
     {
       const double n = pl->geo.real_size;
       g.useful_ratio = (n * n) / ((double)ots::kStream2dWidth * c.ntx * c.nseg *
-                                  (double)(c.zseg + 2 * c.T));
+                                  (double)(c.zseg + 2 * c.R * c.T));
     }
-    if (pl->K->stream2d_attr[c.T] && pl->K->stream2d_attr[c.T](&a) == cudaSuccess)
-      g.registers = a.numRegs;
+    auto attr = c.generic ? pl->K->stream2dg_attr[c.T] : pl->K->stream2d_attr[c.T];
+    if (attr && attr(&a) == cudaSuccess) g.registers = a.numRegs;
     g.ctas_per_sm = c.warps_per_sm / (ots::kStream2dThreads / 32);
   } else if (g.kernel == OTS_KERNEL_STREAM) {
     const StreamCfg& c = pl->scfg;
@@ -674,17 +684,33 @@ ots_status enqueue_run(ots_plan* pl, int kernel) {
         ots_status st = derive_stream2d(pl, Tl, &c);
         if (st != OTS_OK) return st;
       }
-      ots::Stream2dParams sp{};
-      sp.in = pl->state[pl->cur][0];
-      sp.out = pl->state[pl->cur ^ 1][0];
-      sp.aux = pl->info->na ? pl->aux[0] : nullptr;
-      sp.L = pl->L;
-      sp.ntx = c.ntx;
-      sp.nseg = c.nseg;
-      sp.zseg = c.zseg;
-      sp.base_step = base;
-      sp.op = pl->op;
-      e = pl->K->stream2d[Tl](sp, dim3(c.grid), pl->stream);
+      if (c.generic) {
+        ots::Stream2dgParams sp{};
+        for (int f = 0; f < pl->info->ns; ++f) {
+          sp.in[f] = pl->state[pl->cur][f];
+          sp.out[f] = pl->state[pl->cur ^ 1][f];
+        }
+        for (int a = 0; a < pl->info->na; ++a) sp.aux[a] = pl->aux[a];
+        sp.L = pl->L;
+        sp.ntx = c.ntx;
+        sp.nseg = c.nseg;
+        sp.zseg = c.zseg;
+        sp.base_step = base;
+        sp.op = pl->op;
+        e = pl->K->stream2dg[Tl](sp, dim3(c.grid), pl->stream);
+      } else {
+        ots::Stream2dParams sp{};
+        sp.in = pl->state[pl->cur][0];
+        sp.out = pl->state[pl->cur ^ 1][0];
+        sp.aux = pl->info->na ? pl->aux[0] : nullptr;
+        sp.L = pl->L;
+        sp.ntx = c.ntx;
+        sp.nseg = c.nseg;
+        sp.zseg = c.zseg;
+        sp.base_step = base;
+        sp.op = pl->op;
+        e = pl->K->stream2d[Tl](sp, dim3(c.grid), pl->stream);
+      }
       pl->cur ^= 1;
     }
   } else if (kernel == OTS_KERNEL_STREAM) {

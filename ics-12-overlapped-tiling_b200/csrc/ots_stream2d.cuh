@@ -219,4 +219,188 @@ __global__ void __launch_bounds__(kStream2dThreads)
   stream2d_body<Op, T, kLoadLdg>(p, w % p.ntx, w / p.ntx);
 }
 
+// ------------------------------------------------------------------------
+// Generic y-streamed kernel: any 2D stencil, through the op's own apply().
+//
+// Radius R = Op::RY rows: level t works on row k - R t, and each level keeps
+// its 2R+1 newest rows of every state field in registers.  The op reads its
+// neighbourhood through RingAcc, which maps (field, dy, dx) onto those rows
+// at compile time; cells up to RX = Op::RX to the left/right of a lane's
+// four come from the neighbouring lanes (shuffled once per row and level).
+// Aux fields are read at the cell only (every 2D op here does).  The x halo
+// is R T rounded up to 4, so strips hold 128 - 2 roundup4(R T) output cells.
+// ------------------------------------------------------------------------
+struct Stream2dgParams {
+  const float* in[3];
+  float* out[3];
+  const float* aux[2];
+  Layout L;
+  int ntx, nseg, zseg, base_step;
+  OpArgs op;
+};
+
+template <int NS, int D, int RX, int PH, int R>
+struct RingAcc {
+  static constexpr int V = 4;
+  const float (&ring)[NS][D][V];
+  const float (&lh)[NS][D][RX];  // left lane's last RX cells of each row
+  const float (&rh)[NS][D][RX];  // right lane's first RX cells
+  int v, gx, q, nx, ny;
+  __device__ __forceinline__ float operator()(int f, int, int dy, int dx) const {
+    const int s = (PH + dy - R + 2 * D) % D;  // row q + dy of the previous level
+    const int vv = v + dx;
+    if (vv < 0) return lh[f][s][vv + RX];
+    if (vv >= V) return rh[f][s][vv - V];
+    return ring[f][s][vv];
+  }
+  __device__ __forceinline__ bool inside(int, int dy, int dx) const {
+    return (unsigned)(gx + v + dx) < (unsigned)nx && (unsigned)(q + dy) < (unsigned)ny;
+  }
+  __device__ __forceinline__ int gy() const { return q; }
+};
+
+template <int N>
+struct PhaseG {
+  static constexpr int value = N;
+};
+
+template <class Op, int T>
+__global__ void __launch_bounds__(kStream2dThreads)
+    stream2dg_kernel(const __grid_constant__ Stream2dgParams p) {
+  constexpr int V = 4, NS = Op::NS, NA = Op::NA, R = Op::RY, RX = Op::RX, D = 2 * R + 1;
+  constexpr int HX = (R * T + 3) / 4 * 4;
+  constexpr int RPBX = kStream2dWidth - 2 * HX;
+  static_assert(RX <= V && RPBX >= 4, "stencil reach / depth");
+  const int w = blockIdx.x * (kStream2dThreads / 32) + (threadIdx.x >> 5);
+  if (w >= p.ntx * p.nseg) return;  // whole warps only
+  const int strip = w % p.ntx, seg = w / p.ntx;
+  const int lane = threadIdx.x & 31;
+  const int nx = p.L.n0, ny = p.L.n1;
+  const int64_t sy = p.L.sy;
+  const int gx = strip * RPBX - HX + V * lane;  // multiple of 4
+  unsigned xin = 0;
+#pragma unroll
+  for (int v = 0; v < V; ++v)
+    if ((unsigned)(gx + v) < (unsigned)nx) xin |= 1u << v;
+  const bool xall = xin == 0xFu;
+  const bool wx = V * lane >= HX && V * lane < HX + RPBX;
+  const int ys = seg * p.zseg;
+  const int ye = min(ny, ys + p.zseg);
+  const int kb = ys - R * T;
+  const int nit = (ye + R * T - 1) - kb + 1;
+
+  auto load4 = [&](const float* base, int k, float (&d)[V]) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) d[v] = 0.0f;
+    if ((unsigned)k < (unsigned)ny) {
+      const float* src = base + (int64_t)k * sy + gx;
+      if (xall) {
+        const float4 a = __ldg(reinterpret_cast<const float4*>(src));
+        d[0] = a.x; d[1] = a.y; d[2] = a.z; d[3] = a.w;
+      } else {
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+          if ((xin >> v) & 1) d[v] = __ldg(src + v);
+      }
+    }
+  };
+
+  float Rg[T][NS][D][V];  // level t (0 = input): 2R+1 newest rows of every field
+#pragma unroll
+  for (int t = 0; t < T; ++t)
+#pragma unroll
+    for (int f = 0; f < NS; ++f)
+#pragma unroll
+      for (int s = 0; s < D; ++s)
+#pragma unroll
+        for (int v = 0; v < V; ++v) Rg[t][f][s][v] = 0.0f;
+  float P[D][NS][V];  // input rows k .. k + D - 1, fetched ahead
+#pragma unroll
+  for (int j = 0; j < D; ++j)
+#pragma unroll
+    for (int f = 0; f < NS; ++f) load4(p.in[f], kb + j, P[j][f]);
+
+  auto step = [&](auto ph, int r) {
+    constexpr int PH = decltype(ph)::value;  // slot of the newest row
+    const int k = kb + r;
+#pragma unroll
+    for (int f = 0; f < NS; ++f) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) Rg[0][f][PH][v] = P[PH][f][v];
+      load4(p.in[f], k + D, P[PH][f]);
+    }
+#pragma unroll
+    for (int t = 1; t <= T; ++t) {
+      const int q = k - R * t;
+      float lh[NS][D][RX], rh[NS][D][RX];
+#pragma unroll
+      for (int f = 0; f < NS; ++f)
+#pragma unroll
+        for (int s = 0; s < D; ++s)
+#pragma unroll
+          for (int j = 0; j < RX; ++j) {
+            lh[f][s][j] = __shfl_up_sync(0xffffffffu, Rg[t - 1][f][s][V - RX + j], 1);
+            rh[f][s][j] = __shfl_down_sync(0xffffffffu, Rg[t - 1][f][s][j], 1);
+          }
+      const bool qin = (unsigned)q < (unsigned)ny;
+      float res[V][NS];
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        float av[NA > 0 ? NA : 1];
+#pragma unroll
+        for (int a = 0; a < NA; ++a)
+          av[a] = (qin && ((xin >> v) & 1)) ? __ldg(p.aux[a] + (int64_t)q * sy + gx + v) : 0.0f;
+        const RingAcc<NS, D, RX, PH, R> acc{Rg[t - 1], lh, rh, v, gx, q, nx, ny};
+        Op::apply(acc, av, p.op, p.base_step + t - 1, res[v]);
+        if (!(qin && ((xin >> v) & 1))) {  // the Dirichlet ring stays zero
+#pragma unroll
+          for (int f = 0; f < NS; ++f) res[v][f] = 0.0f;
+        }
+      }
+      if (t < T) {
+#pragma unroll
+        for (int f = 0; f < NS; ++f)
+#pragma unroll
+          for (int v = 0; v < V; ++v) Rg[t < T ? t : 0][f][PH][v] = res[v][f];
+      } else if (q >= ys && q < ye && wx) {
+#pragma unroll
+        for (int f = 0; f < NS; ++f) {
+          float* dst = p.out[f] + (int64_t)q * sy + gx;
+          if (xall) {
+            *reinterpret_cast<float4*>(dst) = make_float4(res[0][f], res[1][f], res[2][f], res[3][f]);
+          } else {
+#pragma unroll
+            for (int v = 0; v < V; ++v)
+              if ((xin >> v) & 1) dst[v] = res[v][f];
+          }
+        }
+      }
+    }
+  };
+
+  int r = 0;
+  if constexpr (D == 3) {
+    for (; r + 2 < nit; r += 3) {
+      step(PhaseG<0>{}, r);
+      step(PhaseG<1>{}, r + 1);
+      step(PhaseG<2>{}, r + 2);
+    }
+    if (r < nit) step(PhaseG<0>{}, r++);
+    if (r < nit) step(PhaseG<1>{}, r++);
+  } else {
+    static_assert(D == 5, "radius 1 or 2");
+    for (; r + 4 < nit; r += 5) {
+      step(PhaseG<0>{}, r);
+      step(PhaseG<1>{}, r + 1);
+      step(PhaseG<2>{}, r + 2);
+      step(PhaseG<3>{}, r + 3);
+      step(PhaseG<4>{}, r + 4);
+    }
+    if (r < nit) step(PhaseG<0>{}, r++);
+    if (r < nit) step(PhaseG<1>{}, r++);
+    if (r < nit) step(PhaseG<2>{}, r++);
+    if (r < nit) step(PhaseG<3>{}, r++);
+  }
+}
+
 }  // namespace ots

@@ -32,6 +32,10 @@ def space(stencil, dims, quick=False):
             # y-streamed kernel: T and rows per segment (by; 1 = the library's choice)
             for T, by in itertools.product(range(1, 9), (1, 16, 32, 64, 128)):
                 cfgs.append(dict(kernel="stream", T=T, bx=32, by=by, bz=1, E=1))
+        else:
+            # the generic y-streamed kernel (the op's apply on register rows)
+            for T, by in itertools.product(range(1, 7), (1, 16, 64)):
+                cfgs.append(dict(kernel="stream", T=T, bx=32, by=by, bz=1, E=1))
     else:
         for T, (bx, by, bz), E in itertools.product(
                 range(1, 5), ((32, 4, 4), (32, 8, 2), (64, 4, 2), (16, 8, 4), (16, 16, 2)),

@@ -228,14 +228,29 @@ def test_stream2d_kernel_matches_oracle(st, T):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("st,variant", [("fdtd-2d", 0), ("fdtd-2d", 1), ("rician-denoise-2d", 0),
+                                        ("cdsc-tv-update-2d", 0), ("poisson-2d", 1)])
+@pytest.mark.parametrize("T", [1, 2, 3, 4, 6])
+def test_stream2d_generic_matches_oracle(st, variant, T):
+    # the op's own apply() on register rows: several fields (FDTD and its
+    # row-0 source), radius 2 (Rician), diagonal neighbours and two aux fields
+    # (TV), the 9-point reference Poisson
+    g = run_and_check(st, 150, 2 * T + 1, T=T, bx=32, by=1, E=1, kernel="stream",
+                      variant=variant)
+    assert g.kernel == ots.KERNEL_STREAM
+
+
+@pytest.mark.gpu
 def test_stream2d_small_and_edge_grids():
     for n, steps, T in ((5, 3, 2), (128, 9, 4), (129, 7, 8), (1000, 13, 6)):
         run_and_check("jacobi-2d", n, steps, T=T, bx=32, by=1, E=1, kernel="stream")
     for steps in (0, 1):
         run_and_check("jacobi-2d", 64, steps, T=4, bx=32, by=1, E=1, kernel="stream")
+    for st, n, steps, T in (("rician-denoise-2d", 7, 5, 3), ("fdtd-2d", 129, 11, 4),
+                            ("cdsc-tv-update-2d", 300, 7, 6)):
+        run_and_check(st, n, steps, T=T, bx=32, by=1, E=1, kernel="stream")
     with pytest.raises(ots.OtsError) as ei:
-        ots.Plan("poisson-2d", 64, 4, T=2, bx=32, by=1, E=1, kernel="stream",
-                 variant=ots.VARIANT_REF)
+        ots.Plan("fdtd-2d", 64, 8, T=7, bx=32, by=1, E=1, kernel="stream")
     assert ei.value.status_name == "UNSUPPORTED"
 
 
