@@ -65,5 +65,6 @@ def test_committed_b200_picker_report():
     for s in stencils:
         assert rep[s]["picked_over_best"] >= 0.95, s
     m = rep["_mean"]
-    assert m["picked_over_best"] > m["random_k_over_best"]
-    assert m["top1_over_best"] > m["random_k_over_best"]
+    assert m["picked_over_best"] > m["random_k_over_best"]  # the protocol's comparison
+    assert m["measure_cost"] <= 0.10
+    assert m["top1_over_best"] > m["median_over_best"]
