@@ -15,6 +15,7 @@
 
 #include "ots_stream.cuh"
 #include "ots_stream2d.cuh"
+#include "ots_stream1d.cuh"
 #include "ots_tile.cuh"
 
 namespace ots {
@@ -32,6 +33,8 @@ using AttrFn = cudaError_t (*)(cudaFuncAttributes*);
 using Stream2dLaunch = cudaError_t (*)(const Stream2dParams&, dim3, cudaStream_t);
 using Stream2dgLaunch = cudaError_t (*)(const Stream2dgParams&, dim3, cudaStream_t);
 constexpr int kMaxTg = 6;  // generic 2D stream kernel levels
+using Stream1dLaunch = cudaError_t (*)(const Stream1dParams&, dim3, cudaStream_t);
+constexpr int kStream1dVs[3] = {4, 8, 16};  // cells per lane of the 1D register kernel
 using Occ2dFn = cudaError_t (*)(int*);
 // stream kernel queries take the cluster flag (the clustered instantiation)
 using StreamAttrFn = cudaError_t (*)(cudaFuncAttributes*, bool);
@@ -54,6 +57,8 @@ struct StencilKernels {
   Stream2dgLaunch stream2dg[kMaxTg + 1] = {};  // [T], any 2D stencil through apply()
   AttrFn stream2dg_attr[kMaxTg + 1] = {};
   Occ2dFn stream2dg_occ[kMaxTg + 1] = {};
+  Stream1dLaunch stream1d[3] = {};  // [index of V in kStream1dVs]
+  AttrFn stream1d_attr[3] = {};
 };
 
 template <class K>
@@ -177,6 +182,17 @@ cudaError_t occ_stream2d(int* blocks) {
                                                        kStream2dThreads, 0);
 }
 
+template <class Op, int V>
+cudaError_t launch_stream1d(const Stream1dParams& p, dim3 g, cudaStream_t s) {
+  stream1d_kernel<Op, V><<<g, kStream1dThreads, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+template <class Op, int V>
+cudaError_t attr_stream1d(cudaFuncAttributes* a) {
+  return cudaFuncGetAttributes(a, stream1d_kernel<Op, V>);
+}
+
 template <class Op, int T>
 cudaError_t launch_stream2dg(const Stream2dgParams& p, dim3 g, cudaStream_t s) {
   stream2dg_kernel<Op, T><<<g, kStream2dThreads, 0, s>>>(p);
@@ -226,7 +242,15 @@ void fill_stream_e(StencilKernels& k, std::integer_sequence<int, Ts...>) {
 template <class Op>
 StencilKernels make_kernels() {
   StencilKernels k;
-  if constexpr (Op::DIMS == 1) fill_tile<Op, 0>(k, std::make_integer_sequence<int, kMaxE>{});
+  if constexpr (Op::DIMS == 1) {
+    fill_tile<Op, 0>(k, std::make_integer_sequence<int, kMaxE>{});
+    k.stream1d[0] = &launch_stream1d<Op, 4>;
+    k.stream1d[1] = &launch_stream1d<Op, 8>;
+    k.stream1d[2] = &launch_stream1d<Op, 16>;
+    k.stream1d_attr[0] = &attr_stream1d<Op, 4>;
+    k.stream1d_attr[1] = &attr_stream1d<Op, 8>;
+    k.stream1d_attr[2] = &attr_stream1d<Op, 16>;
+  }
   if constexpr (Op::DIMS == 2) fill_tile<Op, 1>(k, std::make_integer_sequence<int, kMaxE>{});
   if constexpr (Op::DIMS == 2 && Op::NS == 1)
     fill_tex<Op>(k, std::make_integer_sequence<int, kTexMaxE>{});

@@ -163,6 +163,11 @@ EncodeTiledFn encode_tiled() {
   return fn;
 }
 
+// 1D register kernel: warps of 32 x V cells, T steps in registers
+struct Stream1dCfg {
+  int V = 0, vidx = 0, hx = 0, rpb = 0, nw = 0, grid = 0;
+};
+
 // y-streamed 2D kernel: 128-cell strips x y segments, one warp each
 struct Stream2dCfg {
   int T = 0, hx = 0, rpbx = 0, ntx = 0, nseg = 0, zseg = 0, grid = 0;
@@ -211,6 +216,7 @@ struct ots_plan {
   bool tex_ok = false;
   StreamCfg scfg;
   Stream2dCfg s2cfg;
+  Stream1dCfg s1cfg;
   // tile kernel launch shape
   dim3 tile_grid, tile_block;
   size_t tile_smem = 0;
@@ -338,6 +344,28 @@ ots_status derive(const ots_params* p, ots_geometry* g, const StencilInfo** info
 // 2D stream kernel: strips of 128 cells along x (x halo T rounded up to 4 per side), rows split
 // into segments (block_y > 1: that many rows per segment; else
 // stream2d_zseg's choice).
+// 1D: E = cells per lane (4, 8 or 16); the strip keeps 32 E - 2 roundup4(R T)
+// output cells (multiple of 4); the same strips serve shallower launches.
+ots_status derive_stream1d(const ots_plan* pl, Stream1dCfg* c) {
+  const ots_params& p = pl->prm;
+  c->vidx = -1;
+  for (int i = 0; i < 3; ++i)
+    if (ots::kStream1dVs[i] == p.elements_per_thread) c->vidx = i;
+  if (c->vidx < 0 || !pl->K || !pl->K->stream1d[c->vidx])
+    return fail(OTS_ERR_UNSUPPORTED, "1D stream kernel supports E in {4, 8, 16} (got %d)",
+                p.elements_per_thread);
+  c->V = p.elements_per_thread;
+  c->rpb = ots::stream1d_rpb(c->V, pl->info->rx, p.time_tile, &c->hx);
+  if (c->rpb < 4)
+    return fail(OTS_ERR_INVALID_GEOMETRY,
+                "Consistency error! a warp of %d cells leaves no interior at T=%d", 32 * c->V,
+                p.time_tile);
+  c->nw = ceil_div(pl->geo.real_size, c->rpb);
+  const int wpc = ots::kStream1dThreads / 32;
+  c->grid = ceil_div(c->nw, wpc);
+  return OTS_OK;
+}
+
 bool star2d_usable(const ots_plan* pl) {
   return pl->K && pl->K->stream2d[1] &&
          !(pl->prm.stencil == OTS_POISSON_2D && pl->prm.variant == OTS_VARIANT_REF);
@@ -479,7 +507,8 @@ ots_status resolve_kernel(ots_plan* pl, int requested, int* out) {
   if (k == OTS_KERNEL_AUTO)
     k = (star_ok && p.block_z == 1 && p.engine == OTS_ENGINE_NATIVE) ? OTS_KERNEL_STREAM
                                                                       : OTS_KERNEL_TILE;
-  if (k == OTS_KERNEL_STREAM && !star_ok && !star2d_ok)
+  const bool s1_ok = si.dims == 1 && pl->K && pl->K->stream1d[0];
+  if (k == OTS_KERNEL_STREAM && !star_ok && !star2d_ok && !s1_ok)
     return fail(OTS_ERR_UNSUPPORTED,
                 "stream kernel covers the 2D stencils and the 3D star stencils (jacobi-3d, "
                 "poisson-3d in the baseline variant, gradient-3d)");
@@ -571,7 +600,24 @@ void fill_geometry_for_kernel(ots_plan* pl) {
   g.kernel = pl->prm.kernel;
   g.sm_count = pl->sm_count;
   cudaFuncAttributes a{};
-  if (g.kernel == OTS_KERNEL_STREAM && g.dims == 2) {
+  if (g.kernel == OTS_KERNEL_STREAM && g.dims == 1) {
+    const Stream1dCfg& c = pl->s1cfg;
+    g.comps[0] = 32 * c.V;
+    g.comps[1] = g.comps[2] = 1;
+    g.real_per_block[0] = c.rpb;
+    g.real_per_block[1] = g.real_per_block[2] = 1;
+    g.num_blocks[0] = c.nw;
+    g.num_blocks[1] = g.num_blocks[2] = 1;
+    g.threads[0] = 32;  // one warp per strip
+    g.threads[1] = g.threads[2] = 1;
+    g.e_axis = 0;
+    g.shared_bytes = 0;
+    g.useful_ratio = (double)pl->geo.real_size / ((double)32 * c.V * c.nw);
+    if (pl->K->stream1d_attr[c.vidx] && pl->K->stream1d_attr[c.vidx](&a) == cudaSuccess)
+      g.registers = a.numRegs;
+    if (g.registers > 0)
+      g.ctas_per_sm = std::min(32, 65536 / (ots::kStream1dThreads * ((g.registers + 7) / 8 * 8)));
+  } else if (g.kernel == OTS_KERNEL_STREAM && g.dims == 2) {
     const Stream2dCfg& c = pl->s2cfg;
     g.comps[0] = ots::kStream2dWidth;
     g.comps[1] = c.zseg + 2 * c.R * c.T;
@@ -673,6 +719,23 @@ ots_status enqueue_run(ots_plan* pl, int kernel) {
     for (int s = 0; s < S && e == cudaSuccess; ++s) {
       ots::StepParams sp = step_params(pl, pl->cur, s, 1);
       e = pl->K->plain(sp, g, b, 0, pl->stream);
+      pl->cur ^= 1;
+    }
+  } else if (kernel == OTS_KERNEL_STREAM && pl->geo.dims == 1) {
+    const int T = pl->prm.time_tile;
+    const Stream1dCfg& c = pl->s1cfg;
+    for (int base = 0; base < S && e == cudaSuccess; base += T) {
+      ots::Stream1dParams sp{};
+      sp.in = pl->state[pl->cur][0];
+      sp.out = pl->state[pl->cur ^ 1][0];
+      sp.n = pl->L.n0;
+      sp.T = std::min(T, S - base);  // the halo of T covers a shallower last launch
+      sp.base_step = base;
+      sp.rpb = c.rpb;
+      sp.hx = c.hx;
+      sp.nw = c.nw;
+      sp.op = pl->op;
+      e = pl->K->stream1d[c.vidx](sp, dim3(c.grid), pl->stream);
       pl->cur ^= 1;
     }
   } else if (kernel == OTS_KERNEL_STREAM && pl->geo.dims == 2) {
@@ -1022,7 +1085,9 @@ static ots_status prepare(const ots_params* params, ots_plan* pl) {
   st = resolve_kernel(pl, OTS_KERNEL_AUTO, &k);
   if (st != OTS_OK) return st;
   pl->prm.kernel = k;
-  if (k == OTS_KERNEL_STREAM && pl->geo.dims == 2) {
+  if (k == OTS_KERNEL_STREAM && pl->geo.dims == 1) {
+    st = derive_stream1d(pl, &pl->s1cfg);
+  } else if (k == OTS_KERNEL_STREAM && pl->geo.dims == 2) {
     st = derive_stream2d(pl, p.time_tile, &pl->s2cfg);
   } else if (k == OTS_KERNEL_STREAM) {
     st = derive_stream(pl, p.time_tile, &pl->scfg);
@@ -1160,6 +1225,8 @@ ots_status ots_run_async(ots_plan* plan, int32_t kernel) {
     } else if (k == OTS_KERNEL_TEX) {
       st = validate_tile(plan);
       if (st == OTS_OK) st = make_textures(plan);
+    } else if (k == OTS_KERNEL_STREAM && plan->geo.dims == 1) {
+      if (plan->s1cfg.V == 0) st = derive_stream1d(plan, &plan->s1cfg);
     } else if (k == OTS_KERNEL_STREAM && plan->geo.dims == 2) {
       if (plan->s2cfg.T == 0) st = derive_stream2d(plan, plan->prm.time_tile, &plan->s2cfg);
     } else if (k == OTS_KERNEL_STREAM) {

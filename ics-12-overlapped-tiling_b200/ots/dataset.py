@@ -25,6 +25,9 @@ def space(stencil, dims, quick=False):
     if dims == 1:
         for T, bx, E in itertools.product(range(1, 9), (64, 128, 256, 512), (1, 2, 4, 8)):
             cfgs.append(dict(kernel="tile", T=T, bx=bx, by=1, bz=1, E=E))
+        # the register kernel: T steps per launch, E cells per lane
+        for T, E in itertools.product((1, 2, 4, 8, 16, 32, 64), (4, 8, 16)):
+            cfgs.append(dict(kernel="stream", T=T, bx=32, by=1, bz=1, E=E))
     elif dims == 2:
         for T, bx, by, E in itertools.product(range(1, 9), (16, 32, 64), (4, 8, 16), (1, 2, 4, 8)):
             cfgs.append(dict(kernel="tile", T=T, bx=bx, by=by, bz=1, E=E))

@@ -241,6 +241,29 @@ def test_stream2d_generic_matches_oracle(st, variant, T):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("st", ["jacobi-1d", "jacobi-1d-5pt", "jacobi-1d-7pt"])
+@pytest.mark.parametrize("T,E", [(1, 4), (5, 4), (3, 8), (8, 16), (16, 16)])
+def test_stream1d_register_kernel_matches_oracle(st, T, E):
+    # T steps held in registers per warp strip; n not a multiple of the strip
+    # interior, the last launch shallower than T
+    g = run_and_check(st, 100003, 2 * T + 3, T=T, bx=32, by=1, E=E, kernel="stream")
+    assert g.kernel == ots.KERNEL_STREAM and g.threads[0] == 32
+
+
+@pytest.mark.gpu
+def test_stream1d_edges_and_limits():
+    for n, steps, T, E in ((3, 4, 2, 4), (128, 9, 4, 4), (129, 7, 30, 16), (5000, 0, 4, 8),
+                           (5000, 1, 4, 8)):
+        run_and_check("jacobi-1d", n, steps, T=T, bx=32, by=1, E=E, kernel="stream")
+    with pytest.raises(ots.OtsError) as ei:  # 128 cells cannot hold 2 x 90 halo cells
+        ots.Plan("jacobi-1d-7pt", 1000, 60, T=30, bx=32, by=1, E=4, kernel="stream")
+    assert ei.value.status_name == "INVALID_GEOMETRY"
+    with pytest.raises(ots.OtsError) as ei:
+        ots.Plan("jacobi-1d", 1000, 8, T=4, bx=32, by=1, E=2, kernel="stream")
+    assert ei.value.status_name == "UNSUPPORTED"
+
+
+@pytest.mark.gpu
 def test_stream2d_small_and_edge_grids():
     for n, steps, T in ((5, 3, 2), (128, 9, 4), (129, 7, 8), (1000, 13, 6)):
         run_and_check("jacobi-2d", n, steps, T=T, bx=32, by=1, E=1, kernel="stream")
