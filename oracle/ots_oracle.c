@@ -260,6 +260,40 @@ typedef struct {
   float coef, h2;
 } orc_ctx;
 
+/* Rows [0, nrows) of one phase split evenly over the oracle's threads; every
+ * row of a phase is independent, so the result does not depend on the split. */
+typedef void (*orc_rows_fn)(const void* ctx, long r0, long r1);
+typedef struct {
+  orc_rows_fn fn;
+  const void* ctx;
+  long r0, r1;
+} orc_rows_job;
+
+static void* orc_rows_thread(void* p) {
+  const orc_rows_job* j = (const orc_rows_job*)p;
+  j->fn(j->ctx, j->r0, j->r1);
+  return 0;
+}
+
+static void orc_par_rows(orc_rows_fn fn, const void* ctx, long nrows) {
+  int nth = g_orc_threads;
+  if (nth > nrows) nth = (int)nrows;
+  if (nth <= 1) {
+    fn(ctx, 0, nrows);
+    return;
+  }
+  pthread_t th[ORC_MAX_THREADS];
+  orc_rows_job jobs[ORC_MAX_THREADS];
+  for (int k = 0; k < nth; ++k) {
+    jobs[k].fn = fn;
+    jobs[k].ctx = ctx;
+    jobs[k].r0 = nrows * k / nth;
+    jobs[k].r1 = nrows * (k + 1) / nth;
+    pthread_create(&th[k], 0, orc_rows_thread, &jobs[k]);
+  }
+  for (int k = 0; k < nth; ++k) pthread_join(th[k], 0);
+}
+
 static inline int inside3(const orc_ctx* c, int x, int y, int z) {
   if (x < c->lo || x >= c->hi) return 0;
   if (c->dims >= 2 && (y < c->lo || y >= c->hi)) return 0;
