@@ -12,8 +12,10 @@ ranks.
   e2e      the same metric through the public C ABI with host buffers, wall
            clock: each step uploads its dense 512^3 input from page-locked
            memory (ots_upload_interior_async), runs the 100 steps and
-           downloads the result (ots_download_interior_async); two plans
-           alternate so one step's copies overlap the other's kernels.
+           downloads the result (ots_download_interior_async); three plans
+           (--e2e-depth) rotate, so a step's host-to-device copy, the
+           previous step's kernels and the one before's device-to-host copy
+           run at the same time.
   plain    the plain one-step-per-launch kernel, same device timing (the
            comparator of the >= 2x target), reported under "plain".
   roofline HBM: algorithmic bytes per launch (read + write each cell once,
@@ -222,6 +224,140 @@ def run_reference(args):
     return 0
 
 
+def cpu_rate(fn, updates_per_step, max_steps, target_s):
+    """GUpdates/s of `fn(k)` (k steps) on a bounded sample: one step first,
+    then as many steps as fit about `target_s`."""
+    t0 = time.perf_counter()
+    fn(1)
+    one = time.perf_counter() - t0
+    k = max(1, min(max_steps, int(target_s / max(one, 1e-3))))
+    if k == 1:
+        return updates_per_step / one / 1e9, 1, one
+    t0 = time.perf_counter()
+    fn(k)
+    el = time.perf_counter() - t0
+    return updates_per_step * k / el / 1e9, k, el
+
+
+def run_configs(args):
+    """--configs: every workload of ots.workloads at its full size.  Per
+    workload: the exhaustive sweep's best, the learned pick (best measured of
+    the cost model's top 10 %), the plain one-step kernel, the CPU path on one
+    thread (the reference's own loop where it compiles, else the oracle
+    restatement) and on all host threads (bounded samples), and the result of
+    the best configuration checked against the CPU oracle: bit for bit
+    against the FP32 restatement, max / RMS error against the FP64 one.
+    One JSON line per workload on stdout; all of them in --configs-out."""
+    import numpy as np
+    import ots
+    from ots import workloads as W
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O  # the checker and the CPU baselines
+    threads = os.cpu_count() or 1
+    peak, peak_src = peaks()
+    want = None if args.configs == "all" else set(args.configs.split(","))
+    lines = []
+    for w in W.WORKLOADS:
+        st = w["stencil"]
+        if want and st not in want:
+            continue
+        t_start = time.time()
+        done = [0]
+
+        def progress(rec):
+            done[0] += 1
+            if done[0] % 50 == 0:
+                sys.stderr.write("%s: %d configurations, %.0f s\n" % (
+                    w["name"], done[0], time.time() - t_start))
+
+        recs = W.sweep_workload(w, log=progress)
+        ok = [r for r in recs if r.get("status") == "ok"]
+        best = max(ok, key=lambda r: r["gupdates"])
+        cm, cm_desc = W.model_for(st)
+        pk = W.picks(st, recs, cm)
+        cm.close()
+        plain = W.plain_record(w)
+        t_sweep = time.time() - t_start
+        line = {"workload": w["name"], "stencil": st, "n": w["n"], "steps": w["steps"],
+                "space": len(ok), "invalid": len(recs) - len(ok),
+                "exhaustive": {"gupdates": best["gupdates"], "config": W.config_of(best)},
+                "learned": {"gupdates": pk["picked"]["gupdates"],
+                            "config": W.config_of(pk["picked"]), "k": pk["k"],
+                            "over_best": pk["picked"]["gupdates"] / best["gupdates"],
+                            "top1_gupdates": pk["top1"]["gupdates"],
+                            "top1_config": W.config_of(pk["top1"]),
+                            "top1_over_best": pk["top1"]["gupdates"] / best["gupdates"],
+                            "model": cm_desc},
+                "plain": {"gupdates": plain.get("gupdates"), "config": W.config_of(plain)},
+                "speedup_vs_plain": best["gupdates"] / plain["gupdates"]
+                if plain.get("gupdates") else None,
+                "gpu_sweep_seconds": t_sweep}
+        bpu = W.BYTES_PER_UPDATE[st]
+        line["one_step_hbm_roofline"] = {
+            "gupdates": peak / bpu, "bytes_per_update": bpu, "peak_gbs": peak,
+            "peak_source": peak_src, "best_over_roofline": best["gupdates"] / (peak / bpu)}
+        if st == "jacobi-2d":  # the T sweep at 16 x 16 blocks the workload names
+            ts = W.sweep_workload(w, [dict(kernel="tile", T=T, bx=16, by=16, bz=1, E=1)
+                                      for T in range(1, 9)])
+            line["tile_16x16_by_T"] = {str(r["T"]): r.get("gupdates") for r in ts}
+
+        # the best configuration's result against the CPU oracle
+        g, pst, pax, got = W.run_config(w, W.config_of(best))
+        lo, hi = g.padding, g.padding + g.real_size
+        sl = tuple(slice(lo, hi) for _ in range(g.dims))
+        O.set_threads(threads)
+        t0 = time.perf_counter()
+        want32 = O.sweep_f32(st, pst, pax, steps=w["steps"], lo=lo, hi=hi, coef=g.coef, h2=g.h2)
+        t32 = time.perf_counter() - t0
+        bitwise = all(np.array_equal(a[sl].view(np.uint32), b[sl].view(np.uint32))
+                      for a, b in zip(got, want32))
+        del want32
+        t0 = time.perf_counter()
+        want64 = O.sweep_f64(st, pst, pax, steps=w["steps"], lo=lo, hi=hi, coef=g.coef, h2=g.h2)
+        t64 = time.perf_counter() - t0
+        fields = []
+        for a, b in zip(got, want64):
+            mr, rms = O.error_vs_f64(a, b, lo, hi, floor=1e-6)
+            ref_max = float(np.max(np.abs(b[sl])))
+            max_abs = float(np.max(np.abs(a[sl].astype(np.float64) - b[sl])))
+            fields.append({"max_rel": mr, "rms": rms, "max_abs": max_abs,
+                           "max_abs_over_max_ref": max_abs / ref_max if ref_max else None})
+        del want64
+        line["check"] = {"config": W.config_of(best), "bitwise_equal_fp32_oracle": bool(bitwise),
+                         "fp64": fields, "max_rel_floor": 1e-6,
+                         "cpu_seconds": {"fp32": t32, "fp64": t64, "threads": threads}}
+
+        # CPU baselines on bounded samples of the same grid
+        x0 = [a.copy() for a in pst]
+        upd = float(g.interior_points)
+        if st in O.REF_LOOPS and O.ref_available():
+            fn1 = lambda k: O.ref_loop(st, x0[0], g.padding, k)
+            kind = "reference"
+        else:
+            def fn1(k):
+                O.set_threads(1)
+                O.sweep_f32(st, x0, pax, steps=k, lo=lo, hi=hi, coef=g.coef, h2=g.h2)
+            kind = "port"
+        v1, k1, e1 = cpu_rate(fn1, upd, w["steps"], 5.0)
+        O.set_threads(threads)
+        vn, kn, en = cpu_rate(lambda k: O.sweep_f32(st, x0, pax, steps=k, lo=lo, hi=hi,
+                                                    coef=g.coef, h2=g.h2),
+                              upd, w["steps"], 5.0)
+        line["cpu_one_thread"] = {"value": v1, "unit": "GUpdates/s", "cores": 1, "kind": kind,
+                                  "sample": "%d of %d steps (%.1f s)" % (k1, w["steps"], e1)}
+        line["cpu_all_threads"] = {"value": vn, "unit": "GUpdates/s", "cores": threads,
+                                   "kind": "port",
+                                   "sample": "%d of %d steps (%.1f s)" % (kn, w["steps"], en)}
+        line["seconds"] = time.time() - t_start
+        print(json.dumps(line), flush=True)
+        lines.append(line)
+        if args.configs_out:  # rewritten after every workload
+            with open(args.configs_out, "w") as fh:
+                json.dump({"device": ots.device_info(0)["name"], "host_threads": threads,
+                           "workloads": lines}, fh, indent=1)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -230,10 +366,17 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-depth", type=int, default=3,
+                    help="plans in flight in the end-to-end leg (each holds 2 x 537 MB)")
+    ap.add_argument("--configs", help="measure the listed workloads (stencil names, comma "
+                    "separated, or 'all') at full size instead of the bench line")
+    ap.add_argument("--configs-out", help="write the --configs results to this JSON file")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         return run_reference(args)
+    if args.configs:
+        return run_configs(args)
 
     world, rank, local = dist_setup()
     import numpy as np
@@ -312,29 +455,31 @@ def main():
         stream_t1 = None
 
     # end to end through the C ABI with page-locked host buffers: every step
-    # uploads its own input, runs the 100 steps and downloads its result; two
-    # plans alternate, so one problem's copies overlap the other's kernels
+    # uploads its own input, runs the 100 steps and downloads its result; the
+    # plans rotate on their own streams, so the copy engines (one per
+    # direction) and the kernels work on three different problems at once
     # (ots_upload_interior_async / ots_run_async / ots_download_interior_async)
     e2e = None
     if not args.no_e2e:
-        plans = [plan, ots.Plan(STENCIL, N, STEPS, device=local, **cfg)]
+        depth = max(1, args.e2e_depth)
+        plans = [plan] + [ots.Plan(STENCIL, N, STEPS, device=local, **cfg) for _ in range(depth - 1)]
         host_in = [np.ascontiguousarray(a, np.float32) for a in inner[0]]
         aux_in = [np.ascontiguousarray(a, np.float32) for a in inner[1]]
-        host_out = [[np.zeros_like(a) for a in host_in] for _ in range(2)]
+        host_out = [[np.zeros_like(a) for a in host_in] for _ in range(depth)]
         L = ots.lib()
-        pinned = host_in + aux_in + host_out[0] + host_out[1]
+        pinned = host_in + aux_in + [a for o in host_out for a in o]
         for a in pinned:
             ots.check(L.ots_host_register(a.ctypes.data, a.nbytes))
         h2d = sum(a.nbytes for a in host_in + aux_in)
         d2h = sum(a.nbytes for a in host_out[0])
 
         def e2e_step(s):
-            pl = plans[s % 2]
+            pl = plans[s % depth]
             pl.upload_interior_async(host_in, aux_in)
             pl.run_async(cfg["kernel"])
-            pl.download_interior_async(host_out[s % 2])
+            pl.download_interior_async(host_out[s % depth])
 
-        for s in range(2):  # warm-up: both plans once
+        for s in range(depth):  # warm-up: every plan once
             e2e_step(s)
         for pl in plans:
             pl.sync()
@@ -349,14 +494,15 @@ def main():
         t_e2e = reduce_max(time.perf_counter() - t0, world)
         barrier(world)
         same = all(np.array_equal(a.view(np.uint32), b.view(np.uint32))
-                   for a, b in zip(host_out[0], host_out[1]))
+                   for o in host_out[1:] for a, b in zip(host_out[0], o))
         for a in pinned:
             L.ots_host_unregister(a.ctypes.data)
-        plans[1].close()
+        for pl in plans[1:]:
+            pl.close()
         e2e = {"value": job_value(float(N) ** 3 * STEPS * args.steps, world, t_e2e),
                "unit": "GUpdates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-               "pipeline": "two plans alternate on their own streams; each step: upload its "
-                           "input, 100 steps, download its result (wall clock, all copies in)",
+               "pipeline": "%d plans rotate on their own streams; each step: upload its "
+                           "input, 100 steps, download its result (wall clock, all copies in)" % depth,
                "results_identical_across_plans": bool(same)}
 
     peak, peak_src = peaks()

@@ -1,0 +1,205 @@
+"""The measured workloads at their full sizes, their seeded inputs, and the
+three ways of choosing a configuration for each: the learned picker (the cost
+model ranks the space, the top 10 % are measured, the best is kept), the
+exhaustive sweep (every configuration measured) and the plain one-step
+kernel.
+
+Workloads (grid side, time steps):
+
+  jacobi-2d       2048^2,  64 steps   reference fill (srand/rand, uniform [0,1))
+  jacobi-3d        512^3, 100 steps   reference fill, weight 1/7
+  poisson-3d       512^3, 100 steps   reference fill; RHS f = 2 u - 1 (uniform
+                                      [-1,1)), h = 1/(n-1)
+  fdtd-2d         4096^2, 500 steps   reference fill of Ex/Ey/Hz; source row
+  rician-denoise  4096^2, 200 steps   disk image with Rician noise, u0 = f
+  cdsc-tv-update  4096^2, 200 steps   the same image: u0 = F = f, V = 1
+
+The last two are held out: their picks come from a cost model trained without
+them (the reference's leave-one-out protocol, scripts/run-weka.py:74-150).
+
+The disk image: 64 disks of constant intensity (uniform [0.2, 1.0], radius
+uniform [n/64, n/12], centres uniform over the grid, later disks drawn over
+earlier ones) on a 0.1 background; the noisy image is
+f = sqrt((s + n1)^2 + n2^2) with n1, n2 ~ N(0, 0.05^2), the Rician noise model
+whose sigma^2 = 0.0025 the Rician stencil assumes
+(opencl/rician-denoise-2d/rician-denoise-2d.cpp:153-161).  numpy's PCG64
+generator, seeded, makes it reproducible.
+"""
+import json
+import math
+import os
+import time
+
+import numpy as np
+
+from . import OtsError, Plan
+from . import model as M
+from .dataset import space
+from .sweep import make_inputs
+
+WORKLOADS = [
+    dict(name="jacobi-2d 2048^2 x 64", stencil="jacobi-2d", n=2048, steps=64),
+    dict(name="jacobi-3d 512^3 x 100", stencil="jacobi-3d", n=512, steps=100),
+    dict(name="poisson-3d 512^3 x 100", stencil="poisson-3d", n=512, steps=100),
+    dict(name="fdtd-2d 4096^2 x 500", stencil="fdtd-2d", n=4096, steps=500),
+    dict(name="rician-denoise-2d 4096^2 x 200", stencil="rician-denoise-2d", n=4096,
+         steps=200, held_out=True),
+    dict(name="cdsc-tv-update-2d 4096^2 x 200", stencil="cdsc-tv-update-2d", n=4096,
+         steps=200, held_out=True),
+]
+HELD_OUT = ("rician-denoise-2d", "cdsc-tv-update-2d")
+
+# compulsory bytes per update of a one-step launch: read every field once,
+# write every updated field once (FP32)
+BYTES_PER_UPDATE = {"jacobi-2d": 8, "jacobi-3d": 8, "poisson-3d": 12, "fdtd-2d": 24,
+                    "rician-denoise-2d": 12, "cdsc-tv-update-2d": 16}
+
+DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
+
+
+def disk_image(n, seed=2012, count=64, background=0.1, sigma=0.05):
+    """(clean, noisy) n x n float32 images as described in the module doc."""
+    rng = np.random.default_rng(seed)
+    img = np.full((n, n), background, np.float64)
+    yy = np.arange(n, dtype=np.float64)[:, None]
+    xx = np.arange(n, dtype=np.float64)[None, :]
+    for _ in range(count):
+        cx, cy = rng.uniform(0, n, 2)
+        r = rng.uniform(n / 64.0, n / 12.0)
+        val = rng.uniform(0.2, 1.0)
+        y0, y1 = max(0, int(cy - r) - 1), min(n, int(cy + r) + 2)
+        x0, x1 = max(0, int(cx - r) - 1), min(n, int(cx + r) + 2)
+        sub = (yy[y0:y1] - cy) ** 2 + (xx[:, x0:x1] - cx) ** 2 <= r * r
+        img[y0:y1, x0:x1][sub] = val
+    n1 = rng.normal(0.0, sigma, (n, n))
+    n2 = rng.normal(0.0, sigma, (n, n))
+    noisy = np.sqrt((img + n1) ** 2 + n2 ** 2)
+    return img.astype(np.float32), noisy.astype(np.float32)
+
+
+_IMAGES = {}
+
+
+def inputs(plan, seed=123456):
+    """Interior (state, aux) arrays of the workload's inputs for `plan` (its
+    real size may be below the grid side where the reference's size rule
+    truncates; the disk image is then cropped)."""
+    st = plan.stencil
+    if st in HELD_OUT:
+        n = plan.params.problem_size
+        if n not in _IMAGES:
+            _IMAGES[n] = disk_image(n)[1]
+        rs = plan.geometry.real_size
+        f = np.ascontiguousarray(_IMAGES[n][:rs, :rs])
+        if st == "rician-denoise-2d":
+            return [f.copy()], [f]
+        return [f.copy()], [f, np.ones_like(f)]
+    return make_inputs(plan, seed=seed)
+
+
+def measure(plan, kernel, budget_s=0.6):
+    """Median event time (s) of full runs: one warm-up run, then up to three
+    timed runs while they fit `budget_s`.  A configuration whose warm-up run
+    alone takes over a second (far from the best of any space here) keeps
+    that time."""
+    t = plan.run(kernel).event_ms * 1e-3
+    if t > 1.0:
+        return t
+    times = []
+    for _ in range(3):
+        times.append(plan.run(kernel).event_ms * 1e-3)
+        if sum(times) + t > budget_s:
+            break
+    times.sort()
+    return times[len(times) // 2]
+
+
+def sweep_workload(w, cfgs=None, device=0, log=None):
+    """Measure every configuration of the workload's space; returns records
+    with the geometry the model needs."""
+    st, n, steps = w["stencil"], w["n"], w["steps"]
+    dims = 3 if st.endswith("3d") else 2
+    recs = []
+    cache = {}
+    for cfg in cfgs or space(st, dims):
+        rec = dict(stencil=st, n=n, steps=steps, **cfg)
+        try:
+            plan = Plan(st, n, steps, device=device, **cfg)
+        except OtsError as e:
+            rec.update(status=e.status_name)
+            recs.append(rec)
+            continue
+        with plan:
+            g = plan.geometry
+            key = g.real_size
+            if key not in cache:
+                cache.clear()
+                cache[key] = inputs(plan)
+            plan.upload_interior(*cache[key])
+            sec = measure(plan, cfg["kernel"])
+            rec.update(status="ok", seconds=sec,
+                       gupdates=float(g.interior_points) * steps / sec / 1e9,
+                       real_size=g.real_size,
+                       geom={k: (list(v) if hasattr(v, "__len__") else v)
+                             for k, v in g.as_dict().items()})
+        recs.append(rec)
+        if log:
+            log(rec)
+    return recs
+
+
+def model_for(stencil, device=0, epochs=300, seed=0):
+    """The cost model that picks for `stencil`: the shipped model, or for a
+    held-out stencil one trained on the sweep data without both held-out
+    stencils.  Returns (model, description)."""
+    if stencil not in HELD_OUT:
+        with open(os.path.join(DATA, "cost_model.json")) as fh:
+            return M.MLP.from_json(json.load(fh), device=device), "shipped cost model"
+    with open(os.path.join(DATA, "sweeps_b200.json")) as fh:
+        recs = [r for r in json.load(fh)["records"] if r.get("stencil") not in HELD_OUT]
+    X, y, _, _ = M.dataset(recs)
+    m = M.MLP(X.shape[1], 64, 3, seed=seed, device=device)
+    m.fit(X, y, epochs=epochs, seed=seed)
+    return m, "trained without %s" % " and ".join(HELD_OUT)
+
+
+def picks(stencil, recs, cost_model, k_frac=0.10):
+    """The learned pick from measured records: rank every valid
+    configuration, keep the best measured of the top k, and the top-1."""
+    ok = [r for r in recs if r.get("status") == "ok"]
+    if not ok:
+        return None
+    X = np.stack([M.features(stencil, r, r["geom"]) for r in ok])
+    k = max(1, int(math.floor(k_frac * len(ok))))
+    top = [int(i) for i in cost_model.topk(X, k)]
+    best_of_k = max(top, key=lambda i: ok[i]["gupdates"])
+    return {"space": len(ok), "k": k, "picked": ok[best_of_k], "top1": ok[top[0]]}
+
+
+def config_of(rec):
+    return {q: rec[q] for q in ("kernel", "T", "bx", "by", "bz", "E")}
+
+
+def plain_record(w, device=0):
+    """The plain one-step-per-launch kernel on the workload."""
+    cfg = dict(kernel="plain", T=1, bx=32, by=8, bz=1, E=1)
+    return sweep_workload(w, [cfg], device=device)[0]
+
+
+def run_config(w, cfg, device=0):
+    """(plan geometry, padded inputs, padded outputs) of one full run of the
+    workload with `cfg`; the inputs come back padded so a CPU sweep can
+    start from the same state."""
+    with Plan(w["stencil"], w["n"], w["steps"], device=device, **cfg) as plan:
+        g = plan.geometry
+        st, ax = inputs(plan)
+        plan.upload_interior(st, ax)
+        pad = tuple(slice(g.padding, g.padding + g.real_size) for _ in range(g.dims))
+        def padded(a):
+            out = np.zeros((g.padded_size,) * g.dims, np.float32)
+            out[pad] = a
+            return out
+        pst, pax = [padded(a) for a in st], [padded(a) for a in ax]
+        plan.run(cfg["kernel"])
+        got = plan.download()
+        return g, pst, pax, got
