@@ -283,6 +283,7 @@ def run_configs(args):
                 "exhaustive": {"gupdates": best["gupdates"], "config": W.config_of(best)},
                 "learned": {"gupdates": pk["picked"]["gupdates"],
                             "config": W.config_of(pk["picked"]), "k": pk["k"],
+                            "measured": pk["measured"],
                             "over_best": pk["picked"]["gupdates"] / best["gupdates"],
                             "top1_gupdates": pk["top1"]["gupdates"],
                             "top1_config": W.config_of(pk["top1"]),
@@ -311,20 +312,28 @@ def run_configs(args):
         t32 = time.perf_counter() - t0
         bitwise = all(np.array_equal(a[sl].view(np.uint32), b[sl].view(np.uint32))
                       for a, b in zip(got, want32))
-        del want32
+        # the parity tests' metric: max |gpu - cpu| / max(|cpu|, 1)
+        vs32 = max(float(np.max(np.abs(a[sl].astype(np.float64) - b[sl]) /
+                                np.maximum(np.abs(b[sl]), 1.0))) for a, b in zip(got, want32))
         t0 = time.perf_counter()
         want64 = O.sweep_f64(st, pst, pax, steps=w["steps"], lo=lo, hi=hi, coef=g.coef, h2=g.h2)
         t64 = time.perf_counter() - t0
-        fields = []
-        for a, b in zip(got, want64):
-            mr, rms = O.error_vs_f64(a, b, lo, hi, floor=1e-6)
-            ref_max = float(np.max(np.abs(b[sl])))
-            max_abs = float(np.max(np.abs(a[sl].astype(np.float64) - b[sl])))
-            fields.append({"max_rel": mr, "rms": rms, "max_abs": max_abs,
-                           "max_abs_over_max_ref": max_abs / ref_max if ref_max else None})
-        del want64
+
+        def errors(res):
+            out = []
+            for a, b in zip(res, want64):
+                mr, rms = O.error_vs_f64(a, b, lo, hi, floor=1e-6)
+                ref_max = float(np.max(np.abs(b[sl])))
+                max_abs = float(np.max(np.abs(a[sl].astype(np.float64) - b[sl])))
+                out.append({"max_rel": mr, "rms": rms, "max_abs": max_abs,
+                            "max_abs_over_max_ref": max_abs / ref_max if ref_max else None})
+            return out
+
+        fields, fields32 = errors(got), errors(want32)
+        del want32, want64
         line["check"] = {"config": W.config_of(best), "bitwise_equal_fp32_oracle": bool(bitwise),
-                         "fp64": fields, "max_rel_floor": 1e-6,
+                         "max_rel_diff_vs_fp32_oracle": vs32,
+                         "fp64": fields, "fp32_oracle_vs_fp64": fields32, "max_rel_floor": 1e-6,
                          "cpu_seconds": {"fp32": t32, "fp64": t64, "threads": threads}}
 
         # CPU baselines on bounded samples of the same grid

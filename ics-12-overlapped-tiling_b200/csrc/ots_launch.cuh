@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <cstdlib>
 #include <utility>
 
 #include "ots_stream.cuh"
@@ -61,6 +62,45 @@ struct StencilKernels {
   AttrFn stream1d_attr[3] = {};
 };
 
+// Programmatic dependent launch for the launches of a run (the kernels open
+// with grid_dependency_sync()); OTS_PDL=0 in the environment turns it off.
+inline bool launch_overlap() {
+  static const bool on = [] {
+    const char* v = std::getenv("OTS_PDL");
+    return !(v && v[0] == '0');
+  }();
+  return on;
+}
+
+// cudaLaunchKernelEx with the dependent-launch attribute and, for cy > 1,
+// thread-block clusters of cy CTAs along grid y.
+template <class... Exp, class... Act>
+cudaError_t launch_k(void (*kernel)(Exp...), dim3 g, dim3 b, size_t smem, cudaStream_t s,
+                     int cy, Act&&... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = g;
+  cfg.blockDim = b;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[2];
+  unsigned n = 0;
+  if (launch_overlap() && cy <= 1) {  // clustered launches keep plain stream order
+    attr[n].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[n].val.programmaticStreamSerializationAllowed = 1;
+    ++n;
+  }
+  if (cy > 1) {
+    attr[n].id = cudaLaunchAttributeClusterDimension;
+    attr[n].val.clusterDim.x = 1;
+    attr[n].val.clusterDim.y = (unsigned)cy;
+    attr[n].val.clusterDim.z = 1;
+    ++n;
+  }
+  cfg.attrs = attr;
+  cfg.numAttrs = n;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Act>(args)...);
+}
+
 template <class K>
 inline cudaError_t ensure_smem(K kernel, size_t smem, std::atomic<size_t>& cached) {
   if (smem <= 48 * 1024 || smem <= cached.load(std::memory_order_relaxed)) return cudaSuccess;
@@ -75,8 +115,7 @@ cudaError_t launch_tile(const StepParams& p, dim3 g, dim3 b, size_t smem, cudaSt
   static std::atomic<size_t> cached{0};
   cudaError_t e = ensure_smem(tile_kernel<Op, E, EAX>, smem, cached);
   if (e != cudaSuccess) return e;
-  tile_kernel<Op, E, EAX><<<g, b, smem, s>>>(p);
-  return cudaGetLastError();
+  return launch_k(tile_kernel<Op, E, EAX>, g, b, smem, s, 1, p);
 }
 
 template <class Op, int E, int EAX>
@@ -89,8 +128,7 @@ cudaError_t launch_tex(const StepParams& p, dim3 g, dim3 b, size_t smem, cudaStr
   static std::atomic<size_t> cached{0};
   cudaError_t e = ensure_smem(tile_tex_kernel<Op, E>, smem, cached);
   if (e != cudaSuccess) return e;
-  tile_tex_kernel<Op, E><<<g, b, smem, s>>>(p);
-  return cudaGetLastError();
+  return launch_k(tile_tex_kernel<Op, E>, g, b, smem, s, 1, p);
 }
 
 template <class Op, int E>
@@ -100,8 +138,7 @@ cudaError_t attr_tex(cudaFuncAttributes* a) {
 
 template <class Op>
 cudaError_t launch_plain(const StepParams& p, dim3 g, dim3 b, size_t, cudaStream_t s) {
-  plain_kernel<Op><<<g, b, 0, s>>>(p);
-  return cudaGetLastError();
+  return launch_k(plain_kernel<Op>, g, b, 0, s, 1, p);
 }
 
 template <class Op>
@@ -116,25 +153,12 @@ cudaError_t launch_stream(const CUtensorMap& m, const StreamParams& p, dim3 g, d
     static std::atomic<size_t> cached_cl{0};
     cudaError_t e = ensure_smem(stream_kernel<Op, T, E, true>, smem, cached_cl);
     if (e != cudaSuccess) return e;
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = g;
-    cfg.blockDim = b;
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = 1;
-    attr[0].val.clusterDim.y = (unsigned)p.cy;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, stream_kernel<Op, T, E, true>, m, p);
+    return launch_k(stream_kernel<Op, T, E, true>, g, b, smem, s, p.cy, m, p);
   }
   static std::atomic<size_t> cached{0};
   cudaError_t e = ensure_smem(stream_kernel<Op, T, E, false>, smem, cached);
   if (e != cudaSuccess) return e;
-  stream_kernel<Op, T, E, false><<<g, b, smem, s>>>(m, p);
-  return cudaGetLastError();
+  return launch_k(stream_kernel<Op, T, E, false>, g, b, smem, s, 1, m, p);
 }
 
 template <class Op, int T, int E>
@@ -167,8 +191,7 @@ void fill_tile(StencilKernels& k, std::integer_sequence<int, Es...>) {
 
 template <class Op, int T>
 cudaError_t launch_stream2d(const Stream2dParams& p, dim3 g, cudaStream_t s) {
-  stream2d_kernel<Op, T><<<g, kStream2dThreads, 0, s>>>(p);
-  return cudaGetLastError();
+  return launch_k(stream2d_kernel<Op, T>, g, dim3(kStream2dThreads), 0, s, 1, p);
 }
 
 template <class Op, int T>
@@ -184,8 +207,7 @@ cudaError_t occ_stream2d(int* blocks) {
 
 template <class Op, int V>
 cudaError_t launch_stream1d(const Stream1dParams& p, dim3 g, cudaStream_t s) {
-  stream1d_kernel<Op, V><<<g, kStream1dThreads, 0, s>>>(p);
-  return cudaGetLastError();
+  return launch_k(stream1d_kernel<Op, V>, g, dim3(kStream1dThreads), 0, s, 1, p);
 }
 
 template <class Op, int V>
@@ -195,8 +217,7 @@ cudaError_t attr_stream1d(cudaFuncAttributes* a) {
 
 template <class Op, int T>
 cudaError_t launch_stream2dg(const Stream2dgParams& p, dim3 g, cudaStream_t s) {
-  stream2dg_kernel<Op, T><<<g, kStream2dThreads, 0, s>>>(p);
-  return cudaGetLastError();
+  return launch_k(stream2dg_kernel<Op, T>, g, dim3(kStream2dThreads), 0, s, 1, p);
 }
 
 template <class Op, int T>

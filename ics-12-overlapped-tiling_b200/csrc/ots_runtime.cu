@@ -72,6 +72,9 @@ struct StencilInfo {
   int pp_arrays, pp_loads, pp_stores, pp_flops;
   // model constants the runner prints (phase2_global_loads ...); -1 = none
   double r5[8];
+  // the tile step runs in two phases with one float per tile cell of phase-1
+  // values in shared memory (the op's TWO_PHASE form)
+  bool two_phase = false;
 };
 
 // flops: opencl/<s>/<s>.cpp "double gflops" lines (jacobi-2d.cpp:1001-1002,
@@ -91,7 +94,8 @@ const StencilInfo kInfo[OTS_NUM_STENCILS] = {
     {"gradient-2d", 2, 1, 0, 1, 1, 0, 1, true, 15, 1, 5, 1, 18, {5, 0, 12, 5, 1, 1, 1, 4}},
     {"gradient-3d", 3, 1, 0, 1, 1, 1, 1, true, 20, 0, 0, 0, 0, {7, 0, 20, 7, 1, 1, 1, 4}},
     {"fdtd-2d", 2, 3, 0, 1, 1, 0, 1, false, 11, 3, 8, 3, 11, {7, 4, 11, 5, 3, 3, 3, 4}},
-    {"rician-denoise-2d", 2, 1, 1, 2, 2, 0, 1, false, 42, 3, 6, 3, 44, {13, 0, 42, 13, 1, 1, 1, 4}},
+    {"rician-denoise-2d", 2, 1, 1, 2, 2, 0, 1, false, 42, 3, 6, 3, 44, {13, 0, 42, 13, 1, 1, 1, 4},
+     true},
     {"cdsc-tv-update-2d", 2, 1, 2, 1, 1, 0, 1, false, 59, 1, 7, 1, 59, {7, 0, 59, 7, 1, 1, 1, 4}},
     {"cs-3d", 3, 1, 0, 1, 1, 1, 1, false, 65, 0, 0, 0, 0, {-1}},
 };
@@ -582,7 +586,7 @@ ots_status validate_tile(ots_plan* pl) {
                 threads, p.elements_per_thread, fa.maxThreadsPerBlock);
   const StencilInfo& si = *pl->info;
   const int Lx = g.comps[0] + 2 * si.rx, Ly = g.comps[1] + 2 * si.ry, Lz = g.comps[2] + 2 * si.rz;
-  pl->tile_smem = (size_t)2 * si.ns * Lx * Ly * Lz * sizeof(float);
+  pl->tile_smem = (size_t)(2 * si.ns + (si.two_phase ? 1 : 0)) * Lx * Ly * Lz * sizeof(float);
   if (pl->tile_smem > pl->smem_optin)
     return fail(OTS_ERR_SMEM_TOO_LARGE, "Not enough local memory for even one block! (%zu > %zu)",
                 pl->tile_smem, pl->smem_optin);
@@ -669,7 +673,27 @@ void fill_geometry_for_kernel(ots_plan* pl) {
         pl->K->stream_occ[c.T][c.eidx](&b, c.bx * c.by, c.smem, c.cy > 1) == cudaSuccess)
       g.ctas_per_sm = b;
   } else if (g.kernel == OTS_KERNEL_PLAIN) {
+    // one cell per thread, blocks of 256 x 1 (1D) or 32 x 8 x 1, one step
+    // per launch, no shared memory and no redundant cells
+    const int bx = g.dims == 1 ? 256 : 32, by = g.dims == 1 ? 1 : 8;
+    const int n = pl->geo.real_size;
+    g.threads[0] = bx;
+    g.threads[1] = by;
+    g.threads[2] = 1;
+    g.comps[0] = g.real_per_block[0] = bx;
+    g.comps[1] = g.real_per_block[1] = by;
+    g.comps[2] = g.real_per_block[2] = 1;
+    g.num_blocks[0] = ceil_div(n, bx);
+    g.num_blocks[1] = g.dims >= 2 ? ceil_div(n, by) : 1;
+    g.num_blocks[2] = g.dims == 3 ? n : 1;
+    g.e_axis = 0;
+    g.shared_bytes = 0;
+    g.useful_ratio = 1.0;
+    g.launches = pl->prm.time_steps;
     if (pl->K->plain_attr(&a) == cudaSuccess) g.registers = a.numRegs;
+    if (a.numRegs > 0)
+      g.ctas_per_sm = std::max(
+          1, std::min(2048 / (bx * by), 65536 / (bx * by * ((a.numRegs + 7) / 8 * 8))));
   } else {
     const int E = pl->prm.elements_per_thread;
     if (g.kernel == OTS_KERNEL_TEX) {

@@ -242,6 +242,7 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
   uint64_t* hbars = bars + NST;  // [slot][level][side 0 = row from above, 1 = from below]
   const unsigned box_bytes = (unsigned)(TX * TY) * sizeof(float);
   const int n2 = p.L.n2;
+  grid_dependency_sync();
 
   // per-thread constant shared offsets (floats)
   const int lx = V * threadIdx.x, ly = E * threadIdx.y;

@@ -65,6 +65,7 @@ __global__ void __launch_bounds__(kStream1dThreads)
     stream1d_kernel(const __grid_constant__ Stream1dParams p) {
   constexpr int R = Op::RX;
   static_assert(V % 4 == 0 && R <= V, "cells per lane");
+  grid_dependency_sync();
   const int w = blockIdx.x * (kStream1dThreads / 32) + (threadIdx.x >> 5);
   if (w >= p.nw) return;  // whole warps only
   const int lane = threadIdx.x & 31;

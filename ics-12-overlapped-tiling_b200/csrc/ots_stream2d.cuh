@@ -214,6 +214,7 @@ __device__ __forceinline__ void stream2d_body(const Stream2dParams& p, int strip
 template <class Op, int T>
 __global__ void __launch_bounds__(kStream2dThreads)
     stream2d_kernel(const __grid_constant__ Stream2dParams p) {
+  grid_dependency_wait();  // no early trigger: see grid_dependency_sync
   const int w = blockIdx.x * (kStream2dThreads / 32) + (threadIdx.x >> 5);
   if (w >= p.ntx * p.nseg) return;  // whole warps only
   stream2d_body<Op, T, kLoadLdg>(p, w % p.ntx, w / p.ntx);
@@ -271,6 +272,7 @@ __global__ void __launch_bounds__(kStream2dThreads)
   constexpr int HX = (R * T + 3) / 4 * 4;
   constexpr int RPBX = kStream2dWidth - 2 * HX;
   static_assert(RX <= V && RPBX >= 4, "stencil reach / depth");
+  grid_dependency_sync();
   const int w = blockIdx.x * (kStream2dThreads / 32) + (threadIdx.x >> 5);
   if (w >= p.ntx * p.nseg) return;  // whole warps only
   const int strip = w % p.ntx, seg = w / p.ntx;

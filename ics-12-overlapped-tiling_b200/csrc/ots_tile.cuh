@@ -21,9 +21,29 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "ots_ops.cuh"
 
 namespace ots {
+
+// Programmatic dependent launch.  The launches of one run go out with
+// cudaLaunchAttributeProgrammaticStreamSerialization, so launch i+1 can be
+// set up and its CTAs scheduled while launch i drains.  Every stencil kernel
+// opens with this call, before any global memory access: it lets its own
+// successor launch, then waits until its predecessor has completed and that
+// launch's writes are visible.  The ping-pong buffers are therefore never
+// read or written early; without the attribute both instructions are no-ops.
+// Kernels whose grid deliberately fills only part of the GPU (the 2D star
+// stream kernel) only wait: an early trigger there lets the successor's CTAs
+// be placed while most SMs are idle, and they end up unevenly spread.
+__device__ __forceinline__ void grid_dependency_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+__device__ __forceinline__ void grid_dependency_sync() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  grid_dependency_wait();
+}
 
 // Device layout of one field: x fastest, rows of `sy` floats (sy >= n0,
 // 128-byte aligned), planes of `sz` floats.
@@ -87,6 +107,25 @@ struct SmemAcc {
     return in_domain(L, x + dx, y + dy, z + dz);
   }
   __device__ __forceinline__ int gy() const { return y; }
+};
+
+// Phase-1 values of a two-phase stencil (one float per tile cell, the
+// tile's own layout), read at an (dy, dx) offset from the current cell.
+struct SmemGAcc {
+  const float* p;
+  int sy;
+  __device__ __forceinline__ float operator()(int dy, int dx) const { return p[dy * sy + dx]; }
+};
+
+// Ops that provide TWO_PHASE (phase1 + apply2) run the tile step in two
+// phases; every other op keeps its single fused apply().
+template <class Op, class = void>
+struct TwoPhase {
+  static constexpr bool value = false;
+};
+template <class Op>
+struct TwoPhase<Op, std::void_t<decltype(Op::TWO_PHASE)>> {
+  static constexpr bool value = Op::TWO_PHASE;
 };
 
 // Accessor over global memory with zero outside the domain.
@@ -160,6 +199,7 @@ __device__ __forceinline__ void tile_body(const StepParams& p, int bix, int biy,
 
   float* cur = smem;
   float* nxt = smem + NS * Lvol;
+  float* gbuf = smem + 2 * NS * Lvol;  // phase-1 values (two-phase ops only)
   if (p.phase_limit != 3) {
     for (int i = tid; i < Lvol; i += nth) {
       const int lz = i / LxLy;
@@ -206,15 +246,53 @@ __device__ __forceinline__ void tile_body(const StepParams& p, int bix, int biy,
 
   int nsteps = p.steps - p.base_step;
   if (nsteps > T) nsteps = T;
+  // two-phase ops: phase 1 covers the tile minus G_LO cells at the low and
+  // G_HI at the high end of each axis; each thread walks it with a fixed
+  // (x, y) stride, so no cell index is divided inside the loop
+  int gw = 1, gh = 0, g_dx = 0, g_dy = 0, g_x0 = 0, g_y0 = 0;
+  if constexpr (TwoPhase<Op>::value) {
+    gw = Lx - Op::G_LO - Op::G_HI;
+    gh = Ly - Op::G_LO - Op::G_HI;
+    g_dx = nth % gw;
+    g_dy = nth / gw;
+    g_x0 = tid % gw;
+    g_y0 = tid / gw;
+  }
   for (int s = 0; s < nsteps; ++s) {
     float res[E][NS];
+    if constexpr (TwoPhase<Op>::value) {
+      static_assert(Op::DIMS == 2, "two-phase tile step: 2D stencils");
+      for (int gx = g_x0, gy = g_y0; gy < gh;) {
+        const int lx = Op::G_LO + gx, ly = Op::G_LO + gy;
+        const int si = ly * Lx + lx;
+        SmemAcc acc{cur + si, Lvol, Lx, LxLy, ox - RX + lx, oy - RY + ly, oz, p.L};
+        gbuf[si] = Op::phase1(acc);
+        gx += g_dx;
+        gy += g_dy;
+        if (gx >= gw) {
+          gx -= gw;
+          ++gy;
+        }
+      }
+      __syncthreads();
 #pragma unroll
-    for (int e = 0; e < E; ++e) {
-      SmemAcc acc{cur + sidx[e], Lvol, Lx, LxLy, gxs[e], gys[e], gzs[e], p.L};
-      Op::apply(acc, auxv[e], p.op, p.base_step + s, res[e]);
+      for (int e = 0; e < E; ++e) {
+        SmemAcc acc{cur + sidx[e], Lvol, Lx, LxLy, gxs[e], gys[e], gzs[e], p.L};
+        SmemGAcc gacc{gbuf + sidx[e], Lx};
+        Op::apply2(acc, gacc, auxv[e], p.op, p.base_step + s, res[e]);
 #pragma unroll
-      for (int f = 0; f < NS; ++f)
-        if (!ins[e]) res[e][f] = 0.0f;
+        for (int f = 0; f < NS; ++f)
+          if (!ins[e]) res[e][f] = 0.0f;
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        SmemAcc acc{cur + sidx[e], Lvol, Lx, LxLy, gxs[e], gys[e], gzs[e], p.L};
+        Op::apply(acc, auxv[e], p.op, p.base_step + s, res[e]);
+#pragma unroll
+        for (int f = 0; f < NS; ++f)
+          if (!ins[e]) res[e][f] = 0.0f;
+      }
     }
 #pragma unroll
     for (int e = 0; e < E; ++e)
@@ -258,6 +336,7 @@ __device__ __forceinline__ void tile_body(const StepParams& p, int bix, int biy,
 template <class Op, int E, int EAX>
 __global__ void __launch_bounds__(TileThreads<E, Op::NS>::kMax) tile_kernel(const StepParams p) {
   extern __shared__ float smem[];
+  grid_dependency_sync();
   tile_body<Op, E, EAX, kLoadLdg>(p, blockIdx.x, blockIdx.y, blockIdx.z, blockDim.x, blockDim.y,
                                   blockDim.z, threadIdx.x, threadIdx.y, threadIdx.z, smem);
 }
@@ -269,6 +348,7 @@ template <class Op, int E>
 __global__ void __launch_bounds__(TileThreads<E, Op::NS>::kMax) tile_tex_kernel(const StepParams p) {
   static_assert(Op::DIMS == 2 && Op::NS == 1, "texture path: 2D single-field stencils");
   extern __shared__ float smem[];
+  grid_dependency_sync();
   tile_body<Op, E, 1, kLoadTex>(p, blockIdx.x, blockIdx.y, 0, blockDim.x, blockDim.y, 1,
                                 threadIdx.x, threadIdx.y, 0, smem);
 }
@@ -280,6 +360,7 @@ __global__ void __launch_bounds__(TileThreads<E, Op::NS>::kMax) tile_tex_kernel(
 template <class Op>
 __global__ void __launch_bounds__(256) plain_kernel(const StepParams p) {
   constexpr int NS = Op::NS, NA = Op::NA;
+  grid_dependency_sync();
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z * blockDim.z + threadIdx.z;

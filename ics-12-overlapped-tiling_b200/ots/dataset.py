@@ -47,6 +47,10 @@ def space(stencil, dims, quick=False):
         if stencil in ("jacobi-3d", "poisson-3d", "gradient-3d"):
             for T, bx, by, E in itertools.product(range(1, 7), (8, 16, 32), (8, 16, 32), (1, 2, 4)):
                 cfgs.append(dict(kernel="stream", T=T, bx=bx, by=by, bz=1, E=E))
+    # the plain one-step kernel is a candidate too: for compute-bound updates
+    # time tiling buys nothing and one cell per thread can be fastest
+    cfgs.append(dict(kernel="plain", T=1, bx=256 if dims == 1 else 32, by=1 if dims == 1 else 8,
+                     bz=1, E=1))
     if quick:
         cfgs = cfgs[::7]
     return cfgs

@@ -209,8 +209,11 @@ def _mlp_lib():
 
 def dataset(records):
     """(X, y, stencil per row, records) from sweep records with status ok.
-    Target: log GUpdates/s."""
-    rows = [r for r in records if r.get("status") == "ok" and r.get("gupdates", 0) > 0]
+    Target: log GUpdates/s.  The plain one-step kernel is not ranked (the
+    picker always measures it beside the model's picks), so its records are
+    left out."""
+    rows = [r for r in records if r.get("status") == "ok" and r.get("gupdates", 0) > 0
+            and r.get("kernel") != "plain"]
     X = np.stack([features(r["stencil"], r, r["geom"]) for r in rows]) if rows else np.zeros(
         (0, len(FEATURES)), np.float32)
     y = np.log(np.array([r["gupdates"] for r in rows], np.float64)).astype(np.float32)
@@ -232,11 +235,21 @@ def expected_best_of_random(values, k):
     return tot
 
 
+def plain_values(records):
+    """stencil -> measured GUpdates/s of the plain one-step kernel."""
+    return {r["stencil"]: r["gupdates"] for r in records
+            if r.get("kernel") == "plain" and r.get("status") == "ok" and r.get("gupdates", 0) > 0}
+
+
 def leave_one_out(records, k_frac=0.10, hidden=64, layers=3, epochs=300, batch=128, lr=3e-3,
                   weight_decay=1e-4, seed=0, device=0, held_out=None):
-    """Train without stencil s, rank s's space, measure the top k.  Returns a
+    """Train without stencil s, rank s's space, measure the top k -- and the
+    plain one-step kernel, which the picker always measures (one more run):
+    it is the fastest choice for some compute-bound stencils, and a handful
+    of plain records is too few for the model to learn when.  Returns a
     report dict per held-out stencil and the means."""
     X, y, groups, rows = dataset(records)
+    plain = plain_values(records)
     report = {}
     stencils = held_out or sorted(set(groups))
     for s in stencils:
@@ -248,19 +261,22 @@ def leave_one_out(records, k_frac=0.10, hidden=64, layers=3, epochs=300, batch=1
         loss = m.fit(X[tr], y[tr], epochs=epochs, batch=batch, lr=lr, weight_decay=weight_decay,
                      seed=seed)
         actual = np.exp(y[te].astype(np.float64))
+        p = plain.get(s, 0.0)
         k = max(1, int(math.floor(k_frac * len(te))))
         top = m.topk(X[te], k)
-        picked = float(np.max(actual[top]))
-        top1 = float(actual[top[0]])
-        best = float(np.max(actual))
-        rand_k = expected_best_of_random(actual, k)
+        picked = max(float(np.max(actual[top])), p)
+        top1 = max(float(actual[top[0]]), p)
+        best = max(float(np.max(actual)), p)
+        rand_k = expected_best_of_random(np.maximum(actual, p), k)
         pred = m.predict(X[te])
         # rank correlation between predicted and measured
         rp = np.argsort(np.argsort(pred))
         ra = np.argsort(np.argsort(actual))
         spearman = float(np.corrcoef(rp, ra)[0, 1]) if len(te) > 2 else 0.0
-        best_rec = rows[te[int(np.argmax(actual))]]
-        pick_rec = rows[te[int(top[int(np.argmax(actual[top]))])]]
+        plain_rec = {"kernel": "plain", "T": 1, "bx": 0, "by": 0, "bz": 0, "E": 1}
+        best_rec = rows[te[int(np.argmax(actual))]] if np.max(actual) >= p else plain_rec
+        pick_rec = rows[te[int(top[int(np.argmax(actual[top]))])]] if np.max(actual[top]) >= p \
+            else plain_rec
         # the same model ranking the tile-kernel configurations alone (the space
         # the reference's analytical model can rank)
         tile_only = None
@@ -272,8 +288,10 @@ def leave_one_out(records, k_frac=0.10, hidden=64, layers=3, epochs=300, batch=1
             tile_only = {"space": int(len(tsel)), "k": kt,
                          "picked_over_best": float(np.max(at[order[:kt]]) / np.max(at)),
                          "top1_over_best": float(at[order[0]] / np.max(at))}
+        space = len(te) + (1 if s in plain else 0)
         report[s] = {
-            "space": len(te), "k": k, "measure_cost": k / float(len(te)),
+            "space": space, "k": k, "measure_cost": (k + (1 if s in plain else 0)) / float(space),
+            "plain_gupdates": p or None,
             "best_gupdates": best, "picked_gupdates": picked, "picked_over_best": picked / best,
             "top1_over_best": top1 / best, "random_k_over_best": rand_k / best,
             "median_over_best": float(np.median(actual)) / best, "spearman": spearman,

@@ -16,6 +16,8 @@ Workloads (grid side, time steps):
 
 The last two are held out: their picks come from a cost model trained without
 them (the reference's leave-one-out protocol, scripts/run-weka.py:74-150).
+The other seven stencils follow at the sizes the training data was measured
+at (1D 4194304 cells x 64, 2D 2048^2 x 64, 3D 256^3 x 32 steps).
 
 The disk image: 64 disks of constant intensity (uniform [0.2, 1.0], radius
 uniform [n/64, n/12], centres uniform over the grid, later disks drawn over
@@ -46,13 +48,26 @@ WORKLOADS = [
          steps=200, held_out=True),
     dict(name="cdsc-tv-update-2d 4096^2 x 200", stencil="cdsc-tv-update-2d", n=4096,
          steps=200, held_out=True),
+    # the other seven stencils at the training-data sizes, so every stencil
+    # has its FP64 error after the full step count
+    dict(name="jacobi-1d 4194304 x 64", stencil="jacobi-1d", n=1 << 22, steps=64, extra=True),
+    dict(name="jacobi-1d-5pt 4194304 x 64", stencil="jacobi-1d-5pt", n=1 << 22, steps=64,
+         extra=True),
+    dict(name="jacobi-1d-7pt 4194304 x 64", stencil="jacobi-1d-7pt", n=1 << 22, steps=64,
+         extra=True),
+    dict(name="poisson-2d 2048^2 x 64", stencil="poisson-2d", n=2048, steps=64, extra=True),
+    dict(name="gradient-2d 2048^2 x 64", stencil="gradient-2d", n=2048, steps=64, extra=True),
+    dict(name="gradient-3d 256^3 x 32", stencil="gradient-3d", n=256, steps=32, extra=True),
+    dict(name="cs-3d 256^3 x 32", stencil="cs-3d", n=256, steps=32, extra=True),
 ]
 HELD_OUT = ("rician-denoise-2d", "cdsc-tv-update-2d")
 
 # compulsory bytes per update of a one-step launch: read every field once,
 # write every updated field once (FP32)
 BYTES_PER_UPDATE = {"jacobi-2d": 8, "jacobi-3d": 8, "poisson-3d": 12, "fdtd-2d": 24,
-                    "rician-denoise-2d": 12, "cdsc-tv-update-2d": 16}
+                    "rician-denoise-2d": 12, "cdsc-tv-update-2d": 16, "jacobi-1d": 8,
+                    "jacobi-1d-5pt": 8, "jacobi-1d-7pt": 8, "poisson-2d": 12,
+                    "gradient-2d": 8, "gradient-3d": 8, "cs-3d": 8}
 
 DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
 
@@ -118,7 +133,7 @@ def sweep_workload(w, cfgs=None, device=0, log=None):
     """Measure every configuration of the workload's space; returns records
     with the geometry the model needs."""
     st, n, steps = w["stencil"], w["n"], w["steps"]
-    dims = 3 if st.endswith("3d") else 2
+    dims = 1 if st.startswith("jacobi-1d") else 3 if st.endswith("3d") else 2
     recs = []
     cache = {}
     for cfg in cfgs or space(st, dims):
@@ -164,16 +179,20 @@ def model_for(stencil, device=0, epochs=300, seed=0):
 
 
 def picks(stencil, recs, cost_model, k_frac=0.10):
-    """The learned pick from measured records: rank every valid
-    configuration, keep the best measured of the top k, and the top-1."""
-    ok = [r for r in recs if r.get("status") == "ok"]
+    """The learned pick from measured records: rank every valid time-tiled
+    configuration, keep the best measured of the top k and of the plain
+    one-step kernel (always measured), and the model's top-1 (with plain)."""
+    ok = [r for r in recs if r.get("status") == "ok" and r.get("kernel") != "plain"]
+    plain = [r for r in recs if r.get("status") == "ok" and r.get("kernel") == "plain"]
     if not ok:
         return None
     X = np.stack([M.features(stencil, r, r["geom"]) for r in ok])
     k = max(1, int(math.floor(k_frac * len(ok))))
     top = [int(i) for i in cost_model.topk(X, k)]
-    best_of_k = max(top, key=lambda i: ok[i]["gupdates"])
-    return {"space": len(ok), "k": k, "picked": ok[best_of_k], "top1": ok[top[0]]}
+    picked = max([ok[i] for i in top] + plain, key=lambda r: r["gupdates"])
+    top1 = max([ok[top[0]]] + plain, key=lambda r: r["gupdates"])
+    return {"space": len(ok) + len(plain), "k": k, "measured": k + len(plain), "picked": picked,
+            "top1": top1}
 
 
 def config_of(rec):
@@ -182,7 +201,8 @@ def config_of(rec):
 
 def plain_record(w, device=0):
     """The plain one-step-per-launch kernel on the workload."""
-    cfg = dict(kernel="plain", T=1, bx=32, by=8, bz=1, E=1)
+    one_d = w["stencil"].startswith("jacobi-1d")
+    cfg = dict(kernel="plain", T=1, bx=256 if one_d else 32, by=1 if one_d else 8, bz=1, E=1)
     return sweep_workload(w, [cfg], device=device)[0]
 
 

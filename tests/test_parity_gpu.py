@@ -186,6 +186,37 @@ def test_kernel_families_agree_bitwise_on_one_plan():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("st", ["rician-denoise-2d", "cdsc-tv-update-2d"])
+@pytest.mark.parametrize("T,bx,by,E", [(1, 32, 8, 1), (2, 32, 8, 8), (3, 16, 16, 2),
+                                       (4, 64, 8, 4), (2, 16, 4, 3)])
+def test_two_phase_tile_equals_fused_kernels_bitwise(st, T, bx, by, E):
+    """The tile kernel runs Rician in two phases (g stored once per cell in
+    shared memory); the plain kernel and the y-streamed kernel recompute g at
+    every neighbour.  Same operations on the same values: the three agree bit
+    for bit, as they do for TV (fused in every kernel), on the reference fill
+    and on the disk image with Rician noise, with partial edge tiles."""
+    from ots import workloads as W
+    n, steps = 203, 7
+    with ots.Plan(st, n, steps, T=T, bx=bx, by=by, bz=1, E=E, kernel="tile") as plan:
+        g = plan.geometry
+        sl = tuple(slice(g.padding, g.padding + g.real_size) for _ in range(2))
+        fills = [inputs(plan, 3)]
+        f = W.disk_image(g.padded_size, seed=9)[1]
+        img = np.zeros_like(fills[0][0][0])
+        img[sl] = f[sl]
+        fills.append(([img.copy()], [img] if st == "rician-denoise-2d" else
+                      [img, np.where(img != 0, 1.0, 0.0).astype(np.float32)]))
+        for state, aux in fills:
+            outs = []
+            for k in ("tile", "plain", "stream"):
+                plan.upload(state, aux)
+                plan.run(k)
+                outs.append(plan.download()[0])
+            assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32)), "tile vs plain"
+            assert np.array_equal(outs[0].view(np.uint32), outs[2].view(np.uint32)), "tile vs stream"
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("st,n,steps,T,bx,by,E", [
     ("jacobi-2d", 67, 9, 4, 16, 16, 1),
     ("jacobi-2d", 100, 13, 3, 32, 8, 4),

@@ -56,15 +56,23 @@ def test_picks_keep_best_measured_of_top_k():
     scores = np.zeros(len(ok))
     scores[5], scores[6], scores[3] = 3.0, 2.0, 1.0
     p = W.picks("jacobi-2d", recs, _Ranker(scores))
-    assert p["space"] == 20 and p["k"] == 2
+    assert p["space"] == 20 and p["k"] == 2 and p["measured"] == 2
     assert p["top1"]["gupdates"] == 60
     assert p["picked"]["gupdates"] == 70  # best measured of the top 2, not the top-1
     assert W.config_of(p["picked"]) == dict(kernel="tile", T=7, bx=32, by=8, bz=1, E=1)
+    # the plain one-step kernel is not ranked but always measured beside the picks
+    slow = dict(recs[0], kernel="plain", gupdates=65.0)
+    fast = dict(recs[0], kernel="plain", gupdates=95.0)
+    for pl, want in ((slow, 70), (fast, 95)):
+        p = W.picks("jacobi-2d", recs + [pl], _Ranker(scores))
+        assert p["space"] == 21 and p["measured"] == 3
+        assert p["picked"]["gupdates"] == want
 
 
 def test_workload_table_names_every_configured_stencil():
-    names = [w["stencil"] for w in W.WORKLOADS]
+    names = [w["stencil"] for w in W.WORKLOADS if not w.get("extra")]
     assert names == ["jacobi-2d", "jacobi-3d", "poisson-3d", "fdtd-2d", "rician-denoise-2d",
                      "cdsc-tv-update-2d"]
+    assert sorted(w["stencil"] for w in W.WORKLOADS) == sorted(ots.STENCILS)
     assert all(w["stencil"] in W.BYTES_PER_UPDATE for w in W.WORKLOADS)
     assert set(W.HELD_OUT) == {w["stencil"] for w in W.WORKLOADS if w.get("held_out")}
