@@ -187,7 +187,8 @@ def picks(stencil, recs, cost_model, k_frac=0.10):
     if not ok:
         return None
     X = np.stack([M.features(stencil, r, r["geom"]) for r in ok])
-    k = max(1, int(math.floor(k_frac * len(ok))))
+    # the plain runs count against the same budget: k_frac of the space in all
+    k = max(1, int(math.floor(k_frac * (len(ok) + len(plain)))) - len(plain))
     top = [int(i) for i in cost_model.topk(X, k)]
     picked = max([ok[i] for i in top] + plain, key=lambda r: r["gupdates"])
     top1 = max([ok[top[0]]] + plain, key=lambda r: r["gupdates"])
