@@ -201,11 +201,12 @@ __device__ __forceinline__ void tile_body(const StepParams& p, int bix, int biy,
   float* nxt = smem + NS * Lvol;
   float* gbuf = smem + 2 * NS * Lvol;  // phase-1 values (two-phase ops only)
   if (p.phase_limit != 3) {
+    // walk the halo tile with a fixed stride of nth cells, kept as (x, y, z)
+    // digits with carries, so no index is divided inside the loop
+    const int dz = nth / LxLy, dr = nth - dz * LxLy, dy = dr / Lx, dx = dr - dy * Lx;
+    int lz = tid / LxLy, ly = (tid - lz * LxLy) / Lx;
+    int lx = tid - lz * LxLy - ly * Lx;
     for (int i = tid; i < Lvol; i += nth) {
-      const int lz = i / LxLy;
-      const int rem = i - lz * LxLy;
-      const int ly = rem / Lx;
-      const int lx = rem - ly * Lx;
       const int gx = ox - RX + lx, gy = oy - RY + ly, gz = oz - RZ + lz;
       const bool in = in_domain(p.L, gx, gy, gz);
       const int64_t gi = (int64_t)gz * p.L.sz + (int64_t)gy * p.L.sy + gx;
@@ -218,6 +219,17 @@ __device__ __forceinline__ void tile_body(const StepParams& p, int bix, int biy,
           v = in ? tile_load<LD>(p.in[f] + gi) : 0.0f;
         cur[f * Lvol + i] = v;
         nxt[f * Lvol + i] = v;  // the ring of the second buffer stays defined
+      }
+      lx += dx;
+      ly += dy;
+      lz += dz;
+      if (lx >= Lx) {  // dx < Lx and dy < Ly: one carry per digit at most
+        lx -= Lx;
+        ++ly;
+      }
+      if (ly >= Ly) {
+        ly -= Ly;
+        ++lz;
       }
     }
   }

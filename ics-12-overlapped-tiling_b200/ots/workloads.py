@@ -30,7 +30,6 @@ generator, seeded, makes it reproducible.
 import json
 import math
 import os
-import time
 
 import numpy as np
 
