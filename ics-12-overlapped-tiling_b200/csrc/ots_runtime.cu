@@ -215,6 +215,7 @@ struct ots_plan {
   bool clocks_valid = false;  // the last run used the tile kernel
   ots::OpArgs op{};
   CUtensorMap tmap[2];  // stream kernel: field 0 of state buffer 0 / 1
+  CUtensorMap amap;     // stream kernel: aux field 0 (Poisson f), same box
   bool tmap_ok = false;
   cudaTextureObject_t tex[2] = {0, 0};  // texture kernel: field 0 of state buffer 0 / 1
   bool tex_ok = false;
@@ -441,7 +442,7 @@ ots_status derive_stream(const ots_plan* pl, int T, StreamCfg* c) {
     return fail(OTS_ERR_INVALID_GEOMETRY,
                 "Consistency error! stream tile %d x %d leaves no interior at T=%d", c->tx, c->ty,
                 T);
-  c->smem = ots::stream_smem_bytes(T, c->tx, c->ty, c->cy);
+  c->smem = ots::stream_smem_bytes(T, c->tx, c->ty, c->cy, pl->info->na);
   if (c->smem > pl->smem_optin)
     return fail(OTS_ERR_SMEM_TOO_LARGE,
                 "Not enough local memory for even one block! (%zu > %zu bytes)", c->smem,
@@ -825,9 +826,11 @@ ots_status enqueue_run(ots_plan* pl, int kernel) {
       CUtensorMap m;
       if (Tl == pl->scfg.T) {
         m = pl->tmap[pl->cur];
+        if (pl->info->na) sp.amap = pl->amap;
       } else {
         // the last, shallower launch has its own tile box
         ots_status st = make_tmap(pl, c, pl->state[pl->cur][0], &m);
+        if (st == OTS_OK && pl->info->na) st = make_tmap(pl, c, pl->aux[0], &sp.amap);
         if (st != OTS_OK) return st;
       }
       e = pl->K->stream[Tl][c.eidx](m, sp, dim3(c.nbx * c.nby, c.nbz * c.cy, 1), dim3(c.bx, c.by, 1),
@@ -1167,6 +1170,7 @@ ots_status ots_plan_create(const ots_params* params, ots_plan** out) {
   if (k == OTS_KERNEL_STREAM && pl->geo.dims == 3) {
     st = make_tmap(pl, pl->scfg, pl->state[0][0], &pl->tmap[0]);
     if (st == OTS_OK) st = make_tmap(pl, pl->scfg, pl->state[1][0], &pl->tmap[1]);
+    if (st == OTS_OK && pl->info->na) st = make_tmap(pl, pl->scfg, pl->aux[0], &pl->amap);
     if (st != OTS_OK) {
       free_plan(pl);
       return st;
@@ -1258,6 +1262,8 @@ ots_status ots_run_async(ots_plan* plan, int32_t kernel) {
         st = derive_stream(plan, plan->prm.time_tile, &plan->scfg);
         if (st == OTS_OK) st = make_tmap(plan, plan->scfg, plan->state[0][0], &plan->tmap[0]);
         if (st == OTS_OK) st = make_tmap(plan, plan->scfg, plan->state[1][0], &plan->tmap[1]);
+        if (st == OTS_OK && plan->info->na)
+          st = make_tmap(plan, plan->scfg, plan->aux[0], &plan->amap);
         if (st == OTS_OK) plan->tmap_ok = true;
       }
     }

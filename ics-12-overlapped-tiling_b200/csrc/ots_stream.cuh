@@ -18,7 +18,10 @@
 //     and z neighbours), receives z+1 from the level below in registers, and
 //     exchanges x/y neighbours through a double-buffered shared plane per
 //     level; one __syncthreads per plane serves every level;
-//   * level T writes its plane's interior cells straight to global memory.
+//   * level T writes its plane's interior cells straight to global memory;
+//   * a read-only field (Poisson's f) arrives the same way into a second ring
+//     of T + 2 planes, one plane ahead of its first use, so every level reads
+//     its plane's f from shared memory.
 //
 // Every mbarrier wait is bounded; on timeout the CTA records an error word
 // and all its threads leave together (the host reports OTS_ERR_TIMEOUT).
@@ -33,6 +36,7 @@
 namespace ots {
 
 struct StreamParams {
+  CUtensorMap amap;  // the aux field, same box as the state (ops with NA > 0)
   float* out;
   const float* aux;  // star stencils use at most one aux field (Poisson f)
   Layout L;
@@ -161,13 +165,20 @@ __host__ __device__ inline int stream_halo_floats(int T, int TX, int cy) {
   return cy > 1 ? kHaloSlots * T * 2 * TX : 0;
 }
 
+// Planes of the aux ring: level t reads f of plane k - t (t = 1..T) while
+// plane k + 1's copy is in flight.
+__host__ __device__ inline int stream_aux_planes(int T) { return T + 2; }
+
 // Shared bytes: ring + (T-1) double-buffered exchange planes + cluster halo
-// rows + mbarriers (ring stages, and one per halo slot and level).
-__host__ __device__ inline size_t stream_smem_bytes(int T, int TX, int TY, int cy = 1) {
+// rows + aux ring (na > 0) + mbarriers (ring stages, one per halo slot and
+// level, one per aux plane).
+__host__ __device__ inline size_t stream_smem_bytes(int T, int TX, int TY, int cy = 1,
+                                                    int na = 0) {
   size_t plane = (size_t)stream_plane_stride(TX, TY) * sizeof(float);
+  const int nf = na > 0 ? stream_aux_planes(T) : 0;
   return (size_t)kStreamStages * plane + (size_t)(T > 1 ? T - 1 : 0) * 2 * plane +
-         (size_t)stream_halo_floats(T, TX, cy) * sizeof(float) +
-         (size_t)(kStreamStages + kHaloSlots * T * 2) * 8 + 64;
+         (size_t)stream_halo_floats(T, TX, cy) * sizeof(float) + (size_t)nf * plane +
+         (size_t)(kStreamStages + kHaloSlots * T * 2 + nf) * 8 + 64;
 }
 
 // Threads per CTA are capped so that the register rings (3 planes of 4E
@@ -227,6 +238,8 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
   constexpr int V = 4;
   constexpr int HX = StreamGeom<T>::HX, HY = StreamGeom<T>::HY;
   constexpr int NST = kStreamStages, LA = kStreamStages - 2;
+  constexpr bool FR = Op::NA > 0;                  // aux ring
+  constexpr int NF = FR ? T + 2 : 0;               // == stream_aux_planes(T)
   extern __shared__ __align__(128) float smem[];
   const int BX = blockDim.x, BY = blockDim.y;
   const int TX = V * BX, TY = E * BY;
@@ -238,8 +251,10 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
   const int XB = NST * PL;  // exchange planes start (floats)
   const int HB = XB + (T > 1 ? (T - 1) * 2 * PL : 0);  // cluster halo rows start
   float* const hb = smem + HB;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + HB + stream_halo_floats(T, TX, cy));
+  const int FB = HB + stream_halo_floats(T, TX, cy);  // aux ring start (128-byte aligned)
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + FB + NF * PL);
   uint64_t* hbars = bars + NST;  // [slot][level][side 0 = row from above, 1 = from below]
+  uint64_t* fbars = hbars + (cy > 1 ? kHaloSlots * T * 2 : 0);  // one per aux plane
   const unsigned box_bytes = (unsigned)(TX * TY) * sizeof(float);
   const int n2 = p.L.n2;
   grid_dependency_sync();
@@ -266,6 +281,7 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
     for (int s = 0; s < NST; ++s) mbar_init(&bars[s], 1);
     if (cy > 1)
       for (int s = 0; s < kHaloSlots * T * 2; ++s) mbar_init(&hbars[s], 1);
+    for (int s = 0; s < NF; ++s) mbar_init(&fbars[s], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
@@ -312,7 +328,6 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
         xyin |= 1u << (e * V + v);
   const bool xyall = xyin == ((E * V >= 32) ? 0xFFFFFFFFu : ((1u << (E * V)) - 1u));
   float* const obase = p.out + (int64_t)gy * p.L.sy + gx;
-  const float* const abase = p.aux + (int64_t)gy * p.L.sy + gx;
 
   // R[t][slot]: level t's (0 = input) three newest planes of own cells.
   float R[T][3][E][V];
@@ -333,6 +348,11 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
       mbar_arrive_expect_tx(&bars[g & (NST - 1)], box_bytes);
       tma_load_3d(smem + (g & (NST - 1)) * PL, &tmap, tx0, ty0, kb + j, &bars[g & (NST - 1)]);
     }
+    if (FR && nit > 1) {  // f of plane kb, first read at iteration 1
+      const int fs = rg % (NF > 0 ? NF : 1);
+      mbar_arrive_expect_tx(&fbars[fs], box_bytes);
+      tma_load_3d(smem + FB + fs * PL, &p.amap, tx0, ty0, kb, &fbars[fs]);
+    }
   }
 
   auto step = [&](auto ph, int r) -> bool {
@@ -341,7 +361,10 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
     const int k = kb + r;
     const int g = rg + r;  // running plane index: ring stage and phase parity
     const int st = g & (NST - 1);
-    const bool to = !mbar_wait_bounded(&bars[st], (g / NST) & 1, p.err);
+    bool to = !mbar_wait_bounded(&bars[st], (g / NST) & 1, p.err);
+    if (FR && r >= 1 && !to)  // f of plane k - 1, first read by level 1 now
+      to = !mbar_wait_bounded(&fbars[(g - 1) % (NF > 0 ? NF : 1)],
+                              ((g - 1) / (NF > 0 ? NF : 1)) & 1, p.err);
     // cluster halo: the neighbours' rows of plane r-1 (slot of phase hg+r-1)
     const int hr = (hg + r + kHaloSlots - 1) % kHaloSlots;
     const unsigned hpar = (unsigned)((hg + r - 1) / kHaloSlots) & 1u;
@@ -366,6 +389,13 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
       const int s2 = (g + LA) & (NST - 1);
       mbar_arrive_expect_tx(&bars[s2], box_bytes);
       tma_load_3d(smem + s2 * PL, &tmap, tx0, ty0, k + LA, &bars[s2]);
+    }
+    // f of plane k + 1 (read from iteration r + 2 on) into the slot of plane
+    // k + 1 - NF = k - T - 1, whose last reader was level T one iteration ago
+    if (FR && tid == 0 && r + 2 < nit) {
+      const int fs = (g + 1) % (NF > 0 ? NF : 1);
+      mbar_arrive_expect_tx(&fbars[fs], box_bytes);
+      tma_load_3d(smem + FB + fs * PL, &p.amap, tx0, ty0, k + 1, &fbars[fs]);
     }
     // level 0: the input plane k into registers
     const int pk = st * PL;
@@ -418,18 +448,12 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
       }
       const bool zin = (unsigned)q < (unsigned)p.L.n2;
       float fa[E][V];
-      if (Op::NA > 0) {
+      if constexpr (FR) {  // f of plane q from the aux ring (zeros outside the domain)
+        const float* fp = smem + FB + ((g - t + 16 * NF) % NF) * PL + o_row0;
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-          const unsigned m = (xyin >> (e * V)) & 0xF;
-          const float* src = abase + (int64_t)q * p.L.sz + (int64_t)e * p.L.sy;
-          if (zin && m == 0xF) {
-            const float4 f4 = __ldg(reinterpret_cast<const float4*>(src));
-            fa[e][0] = f4.x; fa[e][1] = f4.y; fa[e][2] = f4.z; fa[e][3] = f4.w;
-          } else {
-#pragma unroll
-            for (int v = 0; v < V; ++v) fa[e][v] = (zin && ((m >> v) & 1)) ? __ldg(src + v) : 0.0f;
-          }
+          const float4 f4 = *reinterpret_cast<const float4*>(fp + e * TX);
+          fa[e][0] = f4.x; fa[e][1] = f4.y; fa[e][2] = f4.z; fa[e][3] = f4.w;
         }
       }
       const float tvv[V] = {tv.x, tv.y, tv.z, tv.w};
@@ -541,6 +565,11 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
       // running planes fail_r .. fail_r + LA - 1 were issued
       for (int j = fail_r; j < rg + nit && j < fail_r + LA; ++j)
         mbar_wait_bounded(&bars[j & (NST - 1)], (j / NST) & 1, p.err);
+      // aux planes issued but not yet waited for: up to the failing iteration's
+      // own plane (issued one iteration before it), from its k - 1 on
+      if (FR)
+        for (int j = fail_r - 1; j <= fail_r && j < rg + nit - 1; ++j)
+          if (j >= rg) mbar_wait_bounded(&fbars[j % (NF > 0 ? NF : 1)], (j / (NF > 0 ? NF : 1)) & 1, p.err);
     }
     __syncthreads();
   }
