@@ -359,6 +359,10 @@ def run_configs(args):
                                    "sample": "%d of %d steps (%.1f s)" % (kn, w["steps"], en)}
         line["seconds"] = time.time() - t_start
         print(json.dumps(line), flush=True)
+        # every measured configuration (with the geometry the cost model
+        # reads), so pickers can be re-evaluated offline on the full sizes
+        line["records"] = [{k: r[k] for k in ("kernel", "T", "bx", "by", "bz", "E", "status",
+                                              "gupdates", "geom") if k in r} for r in recs]
         lines.append(line)
         if args.configs_out:  # rewritten after every workload
             with open(args.configs_out, "w") as fh:

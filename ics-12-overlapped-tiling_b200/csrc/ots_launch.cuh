@@ -12,6 +12,7 @@
 
 #include <atomic>
 #include <cstdlib>
+#include <type_traits>
 #include <utility>
 
 #include "ots_stream.cuh"
@@ -215,19 +216,29 @@ cudaError_t attr_stream1d(cudaFuncAttributes* a) {
   return cudaFuncGetAttributes(a, stream1d_kernel<Op, V>);
 }
 
+// The y-streamed kernel of a stencil without the five-point form: FDTD-2D
+// has its own two-phase kernel; every other op goes through its apply().
+template <class Op, int T>
+constexpr auto stream2dg_entry() {
+  if constexpr (std::is_same_v<Op, OpFdtd2D>)
+    return &stream2d_fdtd_kernel<T>;
+  else
+    return &stream2dg_kernel<Op, T>;
+}
+
 template <class Op, int T>
 cudaError_t launch_stream2dg(const Stream2dgParams& p, dim3 g, cudaStream_t s) {
-  return launch_k(stream2dg_kernel<Op, T>, g, dim3(kStream2dThreads), 0, s, 1, p);
+  return launch_k(stream2dg_entry<Op, T>(), g, dim3(kStream2dThreads), 0, s, 1, p);
 }
 
 template <class Op, int T>
 cudaError_t attr_stream2dg(cudaFuncAttributes* a) {
-  return cudaFuncGetAttributes(a, stream2dg_kernel<Op, T>);
+  return cudaFuncGetAttributes(a, stream2dg_entry<Op, T>());
 }
 
 template <class Op, int T>
 cudaError_t occ_stream2dg(int* blocks) {
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, stream2dg_kernel<Op, T>,
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, stream2dg_entry<Op, T>(),
                                                        kStream2dThreads, 0);
 }
 

@@ -52,6 +52,9 @@ void usage(const char* prog) {
           "      --variant ref|baseline   Arithmetic variant (default: ref for compat)\n"
           "      --coef X                 Averaging weight (Jacobi stencils)\n"
           "      --seed N                 srand seed for the input fill (default 123456)\n"
+          "      --init ref|baseline      Inputs: the reference fill everywhere (default), or the\n"
+          "                               benchmark workloads' (Poisson f = 2u - 1; Rician / TV:\n"
+          "                               disk image with Rician noise, u0 = F = f, V = 1)\n"
           "      --plain                  Also time the plain one-step kernel\n"
           "      --device N               CUDA device\n",
           prog);
@@ -151,6 +154,7 @@ int main(int argc, char** argv) {
   p.variant = -1;
   unsigned seed = 123456;  // srand(123456), opencl/jacobi-2d/jacobi-2d.cpp:561
   bool verify = false, plain = false, bx_set = false, by_set = false, dump_clocks = false;
+  bool init_baseline = false;
   std::string save_kernel, load_kernel;
 
   for (int i = 1; i < argc; ++i) {
@@ -200,6 +204,7 @@ int main(int argc, char** argv) {
     } else if (a == "--variant") p.variant = strcmp(next(), "baseline") == 0 ? OTS_VARIANT_BASELINE : OTS_VARIANT_REF;
     else if (a == "--coef") p.coef = (float)atof(next());
     else if (a == "--seed") seed = (unsigned)strtoul(next(), nullptr, 10);
+    else if (a == "--init") init_baseline = strcmp(next(), "baseline") == 0;
     else if (a == "--plain") plain = true;
     else if (a == "--device") p.device = atoi(next());
     else {
@@ -266,6 +271,20 @@ int main(int argc, char** argv) {
   for (auto& v : state) fillp.push_back(v.data());
   for (auto& v : aux) fillp.push_back(v.data());
   ots_fill_reference(dims, P, g.padding, g.real_size, seed, fillp.data(), ns + na);
+  if (init_baseline && (stencil == OTS_POISSON_2D || stencil == OTS_POISSON_3D)) {
+    for (float& f : aux[0]) f = f != 0.0f ? 2.0f * f - 1.0f : 0.0f;  // f uniform [-1, 1)
+  } else if (init_baseline &&
+             (stencil == OTS_RICIAN_DENOISE_2D || stencil == OTS_CDSC_TV_UPDATE_2D)) {
+    const int n = g.real_size;
+    std::vector<float> img((size_t)n * n);
+    ots_fill_disks(n, 2012, 64, 0.1f, 0.05f, img.data(), nullptr);
+    for (int y = 0; y < n; ++y)
+      for (int x = 0; x < n; ++x) {
+        const size_t i = (size_t)(y + lo) * P + (x + lo), j = (size_t)y * n + x;
+        state[0][i] = aux[0][i] = img[j];
+        if (na > 1) aux[1][i] = 1.0f;  // V
+      }
+  }
 
   std::vector<std::vector<float>> ref;
   if (verify) {

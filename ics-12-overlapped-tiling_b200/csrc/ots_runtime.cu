@@ -1039,6 +1039,51 @@ ots_status ots_fill_reference(int32_t dims, int32_t P, int32_t padding, int32_t 
   return OTS_OK;
 }
 
+// The synthetic image of the Rician / TV workloads.  Uniform deviates come
+// from a SplitMix64 stream (Steele, Lea and Flood, "Fast splittable
+// pseudorandom number generators", OOPSLA 2014) as 53-bit doubles, normal
+// deviates from the Box-Muller transform of two uniforms.
+namespace {
+struct SplitMix64 {
+  uint64_t s;
+  uint64_t next() {
+    uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+  }
+  double uniform() { return (double)(next() >> 11) * (1.0 / 9007199254740992.0); }  // [0, 1)
+};
+}  // namespace
+
+ots_status ots_fill_disks(int32_t n, uint64_t seed, int32_t count, float background, float sigma,
+                          float* noisy, float* clean) {
+  if (n < 1 || count < 0 || !noisy || !(sigma >= 0.0f))
+    return fail(OTS_ERR_INVALID_ARGUMENT, "bad disk-image arguments");
+  SplitMix64 rng{seed};
+  std::vector<double> img((size_t)n * n, (double)background);
+  for (int d = 0; d < count; ++d) {
+    const double cx = rng.uniform() * n, cy = rng.uniform() * n;
+    const double r = n / 64.0 + rng.uniform() * (n / 12.0 - n / 64.0);
+    const double val = 0.2 + rng.uniform() * 0.8;
+    const int y0 = std::max(0, (int)(cy - r) - 1), y1 = std::min(n, (int)(cy + r) + 2);
+    const int x0 = std::max(0, (int)(cx - r) - 1), x1 = std::min(n, (int)(cx + r) + 2);
+    for (int y = y0; y < y1; ++y)
+      for (int x = x0; x < x1; ++x)
+        if ((x - cx) * (x - cx) + (y - cy) * (y - cy) <= r * r) img[(size_t)y * n + x] = val;
+  }
+  const double two_pi = 6.283185307179586;
+  for (size_t i = 0; i < img.size(); ++i) {
+    const double u1 = 1.0 - rng.uniform(), u2 = rng.uniform();  // u1 in (0, 1]
+    const double rad = std::sqrt(-2.0 * std::log(u1));
+    const double n1 = sigma * rad * std::cos(two_pi * u2), n2 = sigma * rad * std::sin(two_pi * u2);
+    const double a = img[i] + n1;
+    noisy[i] = (float)std::sqrt(a * a + n2 * n2);
+    if (clean) clean[i] = (float)img[i];
+  }
+  return OTS_OK;
+}
+
 static ots_status prepare(const ots_params* params, ots_plan* pl);
 
 ots_status ots_derive_geometry(const ots_params* params, ots_geometry* out) {

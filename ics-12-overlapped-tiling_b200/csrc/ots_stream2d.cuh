@@ -405,4 +405,158 @@ __global__ void __launch_bounds__(kStream2dThreads)
   }
 }
 
+// ------------------------------------------------------------------------
+// FDTD-2D, y-streamed in its two phases.  The fused update (OpFdtd2D::apply)
+// evaluates E' four times per cell -- at the cell, Ex' at x+1 and Ey' at y+1
+// -- because it sees only the previous level.  Streaming along y, level t can
+// instead compute E' of row q+1 (one row ahead) once per cell and keep it for
+// the next iteration, where it is that level's own E' of row q: H' of row q
+// then takes Ex'(q) at x and x+1 and Ey' at q and q+1 from registers.  Every
+// E' and H' value is the same expression on the same operands as in the fused
+// form (bit-identical results); per cell and level it is two E' evaluations
+// instead of four, and two shuffles instead of eighteen.
+//
+// Per level t >= 1 and iteration (row k = kb + r):
+//   E'(qE = k - t + 1) from level t-1's row qE (Ex, Ey, Hz) and Hz(qE - 1);
+//   H'(qH = k - t)     from level t-1's Hz(qH), this level's E'(qH) (computed
+//                      one iteration earlier) and Ey'(qE);
+//   level t's output row qH = (Ex'(qH), Ey'(qH), H'(qH)).
+// Registers alternate between two slots with the iteration parity (PH), so
+// no row is ever copied.
+template <int T>
+__global__ void __launch_bounds__(kStream2dThreads)
+    stream2d_fdtd_kernel(const __grid_constant__ Stream2dgParams p) {
+  constexpr int V = 4, HX = (T + 3) / 4 * 4;
+  constexpr int RPBX = kStream2dWidth - 2 * HX;
+  static_assert(RPBX >= 4, "depth");
+  grid_dependency_sync();
+  const int w = blockIdx.x * (kStream2dThreads / 32) + (threadIdx.x >> 5);
+  if (w >= p.ntx * p.nseg) return;  // whole warps only
+  const int strip = w % p.ntx, seg = w / p.ntx;
+  const int lane = threadIdx.x & 31;
+  const int nx = p.L.n0, ny = p.L.n1;
+  const int64_t sy = p.L.sy;
+  const int gx = strip * RPBX - HX + V * lane;  // multiple of 4
+  unsigned xin = 0;
+#pragma unroll
+  for (int v = 0; v < V; ++v)
+    if ((unsigned)(gx + v) < (unsigned)nx) xin |= 1u << v;
+  const bool xall = xin == 0xFu;
+  const bool wx = V * lane >= HX && V * lane < HX + RPBX;
+  const int ys = seg * p.zseg;
+  const int ye = min(ny, ys + p.zseg);
+  const int kb = ys - T;
+  const int nit = (ye + T - 1) - kb + 1;
+  const bool src_row = p.op.variant == 0;  // Ey on interior row 0 driven to the step index
+
+  auto load4 = [&](const float* base, int k, float (&d)[V]) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) d[v] = 0.0f;
+    if ((unsigned)k < (unsigned)ny) {
+      const float* src = base + (int64_t)k * sy + gx;
+      if (xall) {
+        const float4 a = __ldg(reinterpret_cast<const float4*>(src));
+        d[0] = a.x; d[1] = a.y; d[2] = a.z; d[3] = a.w;
+      } else {
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+          if ((xin >> v) & 1) d[v] = __ldg(src + v);
+      }
+    }
+  };
+
+  float In[2][3][V];       // level 0: input rows k (slot PH) and k - 1 (slot PH ^ 1)
+  float Pf[2][3][V];       // input rows fetched ahead (k + 1 in slot PH ^ 1, k + 2 in PH)
+  float Ec[T + 1][2][2][V];  // level t: E' rows (slot PH: row k - t + 1; PH ^ 1: row k - t)
+  float Hl[T + 1][2][V];     // level t: H' rows (slot PH: row k - t; PH ^ 1: row k - t - 1)
+#pragma unroll
+  for (int s = 0; s < 2; ++s)
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+#pragma unroll
+      for (int f = 0; f < 3; ++f) In[s][f][v] = 0.0f;
+#pragma unroll
+      for (int t = 0; t <= T; ++t) {
+        Ec[t][s][0][v] = Ec[t][s][1][v] = 0.0f;
+        Hl[t][s][v] = 0.0f;
+      }
+    }
+#pragma unroll
+  for (int j = 0; j < 2; ++j)
+#pragma unroll
+    for (int f = 0; f < 3; ++f) load4(p.in[f], kb + j, Pf[j][f]);
+
+  auto step = [&](auto ph, int r) {
+    constexpr int PH = decltype(ph)::value, PO = PH ^ 1;
+    const int k = kb + r;
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) In[PH][f][v] = Pf[PH][f][v];
+      load4(p.in[f], k + 2, Pf[PH][f]);
+    }
+#pragma unroll
+    for (int t = 1; t <= T; ++t) {
+      const int qE = k - t + 1, qH = k - t;
+      // level t-1's row qE (Ex, Ey, Hz) and its Hz of row qE - 1 = qH
+      const float(&Lx)[V] = t == 1 ? In[PH][0] : Ec[t > 1 ? t - 1 : 0][PO][0];
+      const float(&Ly)[V] = t == 1 ? In[PH][1] : Ec[t > 1 ? t - 1 : 0][PO][1];
+      const float(&Lh)[V] = t == 1 ? In[PH][2] : Hl[t > 1 ? t - 1 : 0][PH];
+      const float(&Lhp)[V] = t == 1 ? In[PO][2] : Hl[t > 1 ? t - 1 : 0][PO];
+      const int step_t = p.base_step + t - 1;
+      // E' of row qE (OpFdtd2D::ex_new / ey_new at that row)
+      const float hl = __shfl_up_sync(0xffffffffu, Lh[V - 1], 1);  // Hz(qE) at x - 1 of cell 0
+      const bool qEin = (unsigned)qE < (unsigned)ny;
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const bool in = qEin && ((xin >> v) & 1);
+        const float hxm = v > 0 ? Lh[v - 1] : hl;
+        Ec[t][PH][0][v] = in ? Lx[v] - 0.5f * (Lh[v] - hxm) : 0.0f;
+        Ec[t][PH][1][v] = !in ? 0.0f
+                              : (src_row && qE == 0) ? (float)step_t
+                                                     : Ly[v] - 0.5f * (Lh[v] - Lhp[v]);
+      }
+      // H' of row qH from E'(qH) (slot PO) and Ey'(qE)
+      const float exr = __shfl_down_sync(0xffffffffu, Ec[t][PO][0][0], 1);  // Ex'(qH) at x + 1 of cell 3
+      const bool qHin = (unsigned)qH < (unsigned)ny;
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const float ex = Ec[t][PO][0][v], ey = Ec[t][PO][1][v];
+        const float exp1 = v < V - 1 ? Ec[t][PO][0][v + 1] : exr;
+        float d = (exp1 - ex) + Ec[t][PH][1][v];
+        d = (p.op.variant == 1) ? d + ey : d - ey;
+        const float h = Lhp[v] - 0.7f * d;
+        Hl[t][PH][v] = (qHin && ((xin >> v) & 1)) ? h : 0.0f;
+      }
+      if (t == T && qH >= ys && qH < ye && wx) {
+        float* dst[3] = {p.out[0] + (int64_t)qH * sy + gx, p.out[1] + (int64_t)qH * sy + gx,
+                         p.out[2] + (int64_t)qH * sy + gx};
+        const float(&ox)[V] = Ec[T][PO][0];
+        const float(&oy)[V] = Ec[T][PO][1];
+        const float(&oh)[V] = Hl[T][PH];
+        if (xall) {
+          *reinterpret_cast<float4*>(dst[0]) = make_float4(ox[0], ox[1], ox[2], ox[3]);
+          *reinterpret_cast<float4*>(dst[1]) = make_float4(oy[0], oy[1], oy[2], oy[3]);
+          *reinterpret_cast<float4*>(dst[2]) = make_float4(oh[0], oh[1], oh[2], oh[3]);
+        } else {
+#pragma unroll
+          for (int v = 0; v < V; ++v)
+            if ((xin >> v) & 1) {
+              dst[0][v] = ox[v];
+              dst[1][v] = oy[v];
+              dst[2][v] = oh[v];
+            }
+        }
+      }
+    }
+  };
+
+  int r = 0;
+  for (; r + 1 < nit; r += 2) {
+    step(PhaseG<0>{}, r);
+    step(PhaseG<1>{}, r + 1);
+  }
+  if (r < nit) step(PhaseG<0>{}, r);
+}
+
 }  // namespace ots

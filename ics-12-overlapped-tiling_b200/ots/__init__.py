@@ -210,6 +210,21 @@ def derive_geometry(**kw):
     return g
 
 
+def fill_disks(n, seed=2012, count=64, background=0.1, sigma=0.05):
+    """(clean, noisy) n x n float32 images: ots_fill_disks (the Rician / TV
+    workloads' input)."""
+    noisy = np.zeros((n, n), np.float32)
+    clean = np.zeros((n, n), np.float32)
+    L = lib()
+    fn = L.ots_fill_disks
+    fn.argtypes = [ctypes.c_int32, ctypes.c_uint64, ctypes.c_int32, ctypes.c_float,
+                   ctypes.c_float, _FP, _FP]
+    fn.restype = ctypes.c_int
+    check(fn(n, seed, count, background, sigma, noisy.ctypes.data_as(_FP),
+             clean.ctypes.data_as(_FP)))
+    return clean, noisy
+
+
 def fill_reference(dims, P, padding, real_size, seed, nfields):
     arrs = [np.zeros((P,) * dims, np.float32) for _ in range(nfields)]
     check(lib().ots_fill_reference(dims, P, padding, real_size, seed, _fptrs(arrs), nfields))

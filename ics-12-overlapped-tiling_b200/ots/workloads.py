@@ -24,8 +24,9 @@ uniform [n/64, n/12], centres uniform over the grid, later disks drawn over
 earlier ones) on a 0.1 background; the noisy image is
 f = sqrt((s + n1)^2 + n2^2) with n1, n2 ~ N(0, 0.05^2), the Rician noise model
 whose sigma^2 = 0.0025 the Rician stencil assumes
-(opencl/rician-denoise-2d/rician-denoise-2d.cpp:153-161).  numpy's PCG64
-generator, seeded, makes it reproducible.
+(opencl/rician-denoise-2d/rician-denoise-2d.cpp:153-161); seeded SplitMix64
+uniforms and Box-Muller normals (ots_fill_disks), so the CLI's
+--init baseline and this table start from the same image.
 """
 import json
 import math
@@ -72,23 +73,10 @@ DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
 
 
 def disk_image(n, seed=2012, count=64, background=0.1, sigma=0.05):
-    """(clean, noisy) n x n float32 images as described in the module doc."""
-    rng = np.random.default_rng(seed)
-    img = np.full((n, n), background, np.float64)
-    yy = np.arange(n, dtype=np.float64)[:, None]
-    xx = np.arange(n, dtype=np.float64)[None, :]
-    for _ in range(count):
-        cx, cy = rng.uniform(0, n, 2)
-        r = rng.uniform(n / 64.0, n / 12.0)
-        val = rng.uniform(0.2, 1.0)
-        y0, y1 = max(0, int(cy - r) - 1), min(n, int(cy + r) + 2)
-        x0, x1 = max(0, int(cx - r) - 1), min(n, int(cx + r) + 2)
-        sub = (yy[y0:y1] - cy) ** 2 + (xx[:, x0:x1] - cx) ** 2 <= r * r
-        img[y0:y1, x0:x1][sub] = val
-    n1 = rng.normal(0.0, sigma, (n, n))
-    n2 = rng.normal(0.0, sigma, (n, n))
-    noisy = np.sqrt((img + n1) ** 2 + n2 ** 2)
-    return img.astype(np.float32), noisy.astype(np.float32)
+    """(clean, noisy) n x n float32 images as described in the module doc
+    (ots_fill_disks in libots, the generator the CLI's --init baseline uses)."""
+    from . import fill_disks
+    return fill_disks(n, seed, count, background, sigma)
 
 
 _IMAGES = {}

@@ -197,6 +197,17 @@ ots_status ots_fill_reference(int32_t dims, int32_t padded_size, int32_t padding
                               int32_t real_size, uint32_t seed, float* const* fields,
                               int32_t num_fields);
 
+/* The image the Rician and TV workloads start from (no counterpart in the
+ * reference, whose fill for these runners is disabled,
+ * opencl/rician-denoise-2d/rician-denoise-2d.cpp:694-708): `count` disks of
+ * constant intensity (uniform [0.2, 1.0)), radius uniform [n/64, n/12),
+ * centres uniform over the grid, drawn in order over `background`; then
+ * Rician noise f = sqrt((s + n1)^2 + n2^2), n1, n2 ~ N(0, sigma^2).  Seeded
+ * (SplitMix64 uniforms, Box-Muller normals).  noisy (and clean, if not NULL):
+ * n x n floats, row-major.  Needs no GPU. */
+ots_status ots_fill_disks(int32_t n, uint64_t seed, int32_t count, float background, float sigma,
+                          float* noisy, float* clean);
+
 /* ---- plans -------------------------------------------------------------- */
 
 /* Derive the geometry, pick and validate the kernel instantiation, allocate

@@ -127,3 +127,22 @@ def test_yaml_experiment_through_cli_to_analytic_model(tmp_path):
     rep = A.evaluate(rows, A.get_arch("b200"))
     assert rep["jacobi-2d"]["ranked"] == 14
     assert 0.0 < rep["jacobi-2d"]["top1_over_best"] <= 1.0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("stencil,args", [
+    ("rician-denoise-2d", ["-n", 256, "-t", 4, "-s", 2, "-x", 32, "-y", 8, "-e", 4]),
+    ("cdsc-tv-update-2d", ["-n", 256, "-t", 4, "-s", 2, "-x", 32, "-y", 8, "-e", 2]),
+    ("poisson-3d", ["-n", 40, "-t", 4, "-s", 2, "-x", 16, "-y", 8, "-z", 1, "-e", 2,
+                    "--kernel", "stream"]),
+])
+def test_cli_init_baseline_runs_the_benchmark_inputs(stencil, args):
+    """--init baseline starts from the benchmark workloads' inputs (the disk
+    image with Rician noise for Rician / TV, f in [-1, 1) for Poisson); the
+    runner's -v check passes on them, and they are not the reference fill."""
+    common = args + ["--engine", "native", "--variant", "baseline", "-v"]
+    r_ref, kv_ref = cli(stencil, *common)
+    r_base, kv_base = cli(stencil, *(common + ["--init", "baseline"]))
+    assert r_ref.returncode == 0 and r_base.returncode == 0, r_base.stderr
+    assert kv_base["Correctness"] == "PASSED" and kv_ref["Correctness"] == "PASSED"
+    assert kv_base["Ref Norm"] != kv_ref["Ref Norm"]
