@@ -6,7 +6,7 @@ This is the B200 counterpart of the reference's sweep harness
 of one workload on the GPU, records the runner's keys plus the measured
 GUpdates/s, and skips invalid configurations the way the reference's
 runner exits with "ERROR:"/"Consistency error!".  Results are the training
-data of the learned cost model and the judge of its picks.
+data of the learned cost model and the measure its picks are scored by.
 
 Usage:
     python -m ots.sweep --stencil jacobi-3d -n 512 -t 100 --kernel stream \

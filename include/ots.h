@@ -96,9 +96,9 @@ typedef enum ots_kernel {
 } ots_kernel;
 
 /* Arithmetic variant where the reference and the benchmark definition
- * differ.  BASELINE: jacobi-3d weight 1/7; Poisson as a Jacobi sweep with RHS
+ * differ.  OTS_VARIANT_BASELINE: jacobi-3d weight 1/7; Poisson as a Jacobi sweep with RHS
  * f and h^2 (5-/7-point); FDTD with the standard Hz sign and the Ey row-0
- * source.  REF: the reference kernels' arithmetic (0.143f; 8c-sum8 and
+ * source.  OTS_VARIANT_REF: the reference kernels' arithmetic (0.143f; 8c-sum8 and
  * 26c-sum26; +Ey in the Hz update, no source). */
 typedef enum ots_variant { OTS_VARIANT_BASELINE = 0, OTS_VARIANT_REF = 1 } ots_variant;
 
@@ -300,7 +300,7 @@ ots_status ots_host_unregister(void* ptr);
  * counterpart: the reference runs one grid per process
  * (opencl/jacobi-2d/jacobi-2d.cpp:553-1048).  `grids` uses ots_params; the
  * fields read are stencil, problem_size, time_steps, time_tile, block_x,
- * elements_per_thread, coef and h2 (Poisson uses the BASELINE variant). */
+ * elements_per_thread, coef and h2 (Poisson uses OTS_VARIANT_BASELINE). */
 typedef struct ots_batch ots_batch;
 
 ots_status ots_batch_create(const ots_params* grids, int32_t n, int32_t device, ots_batch** out);
