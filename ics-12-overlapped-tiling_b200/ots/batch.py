@@ -179,6 +179,9 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=2012)
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--no-model", action="store_true")
+    ap.add_argument("--mode", default="all", choices=["all", "stream-graph", "tile-graph"],
+                    help="all: every comparison; stream-graph / tile-graph: only that one "
+                    "graph-captured launch (e.g. under a profiler)")
     a = ap.parse_args(argv)
     from . import model as M
     cm = None
@@ -186,8 +189,25 @@ def main(argv=None):
         path = os.path.join(os.path.dirname(__file__), "data", "cost_model.json")
         cm = M.MLP.from_json(json.load(open(path)))
     grids = pick(workload(a.grids, a.seed), cm)
-    b = Batch(grids)
     ins = inputs(grids)
+    if a.mode != "all":
+        one = Batch(pick_stream([dict(g) for g in grids]) if a.mode == "stream-graph" else grids)
+        for i, (s, x) in enumerate(ins):
+            one.upload(i, s, x)
+        one.run()  # warm-up
+        ts = []
+        for _ in range(a.reps):
+            for i, (s, x) in enumerate(ins):
+                one.upload(i, s, x)
+            ts.append(one.run())
+        info = one.info()
+        one.close()
+        t = sorted(ts)[len(ts) // 2]
+        print(json.dumps({"metric": "GUpdates/s", "mode": a.mode, "updates": info["updates"],
+                          "items": info["items"], "ctas": info["ctas"],
+                          "value": info["updates"] / t / 1e9, "seconds": t}))
+        return 0
+    b = Batch(grids)
 
     def load():
         for i, (s, x) in enumerate(ins):
