@@ -129,3 +129,28 @@ def test_fp32_sweep_tracks_fp64_sweep(st):
     for x, y in zip(a32, a64):
         mr, rms = O.error_vs_f64(x, y, pad, P - pad, floor=1.0)
         assert mr < 1e-5, (st, mr)
+
+
+@pytest.mark.parametrize("st", sorted(O.SID))
+def test_thread_count_does_not_change_a_bit(st):
+    """The oracle splits every phase by rows (1D: by chunks of the line) over
+    its threads; each cell is computed the same way whatever the split, so one
+    thread and several threads agree bit for bit, in FP32 and FP64.  Sizes
+    cover several 1D chunks and uneven row splits."""
+    d = O.dims(st)
+    n = {1: 40000, 2: 97, 3: 23}[d]
+    pad = 3
+    P = n + 2 * pad
+    ns = O.num_state(st)
+    arrs = O.fill_ref(d, P, pad, P - pad, 17, ns + O.num_aux(st))
+    state, aux = arrs[:ns], arrs[ns:]
+    try:
+        for sweep in (O.sweep_f32, O.sweep_f64):
+            O.set_threads(1)
+            one = sweep(st, state, aux, steps=4, lo=pad, hi=P - pad, h2=1e-4)
+            O.set_threads(7)
+            many = sweep(st, state, aux, steps=4, lo=pad, hi=P - pad, h2=1e-4)
+            for a, b in zip(one, many):
+                assert np.array_equal(a.view(np.uint8), b.view(np.uint8)), (st, sweep.__name__)
+    finally:
+        O.set_threads(1)
