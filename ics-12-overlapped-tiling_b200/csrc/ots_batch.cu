@@ -409,12 +409,20 @@ ots_status ots_batch_create(const ots_params* grids, int32_t n, int32_t device, 
     g.buf[1] = b->pool + off[i] + f;
     g.aux = g.op == 1 ? b->pool + off[i] + 2 * f : nullptr;
   }
-  // work queue in rounds of chunks
+  // work queue in rounds of chunks; within a round the grids go stencil by
+  // stencil, so the warps dequeued together mostly run the same unrolled
+  // pipeline (the instruction cache holds one stencil's code, not three).
+  // Every item waits only for its own grid's previous round, which lies
+  // wholly earlier in the queue, whatever the order inside a round.
   std::vector<int4> items;
   int maxc = 0;
   for (auto& g : b->grids) maxc = std::max(maxc, g.chunks);
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int c) { return b->grids[a].op < b->grids[c].op; });
   for (int r = 0; r < maxc; ++r)
-    for (int i = 0; i < n; ++i)
+    for (int i : order)
       if (b->grids[i].chunks > r)
         for (int t = 0; t < b->grids[i].ntx * b->grids[i].nty; ++t) items.push_back(make_int4(i, r, t, 0));
   b->nitems = (int)items.size();
