@@ -12,7 +12,8 @@
 //   * a CTA takes the next item with one atomicAdd, waits until every tile
 //     of the grid's previous chunk has completed (a per-(grid, chunk)
 //     counter; a bounded spin that records an error and gives up after 2 s
-//     or once another CTA has given up), runs the overlapped tile
+//     or once another CTA has given up; the host can set the limit), runs
+//     the overlapped tile
 //     (tile_body, loads at L2 because other CTAs wrote them), and publishes
 //     its completion (fence, then counter increment);
 //   * per grid, the tile shape (T, block x, E) is its own -- chosen by the
@@ -55,7 +56,12 @@ struct BatchGrid {
   float* buf[2];
   const float* aux;
   OpArgs op_args;
+  uint64_t wait_ns;   // limit of a dependency wait (2 s unless the host sets it)
+  int hold;           // test hook: 1 = chunks >= 1 wait for a count never reached
 };
+
+constexpr uint64_t kBatchWaitNs = 2000000000ull;
+constexpr unsigned kBatchMaxPolls = 1u << 26;  // a second bound, should the timer stall
 
 __device__ __forceinline__ uint64_t batch_ns() {
   uint64_t t;
@@ -91,7 +97,7 @@ __global__ void __launch_bounds__(kBatchThreads) batch_kernel(const BatchGrid* _
     if (threadIdx.x == 0) {
       int ok = *(volatile int*)err == 0;
       if (ok && w.y > 0) {
-        const int need = g.ntx * g.nty;
+        const int need = g.ntx * g.nty + g.hold;
         volatile int* c = counters + g.cnt_off + w.y - 1;
         const uint64_t t0 = batch_ns();
         unsigned i = 0;
@@ -100,7 +106,7 @@ __global__ void __launch_bounds__(kBatchThreads) batch_kernel(const BatchGrid* _
             ok = 0;
             break;
           }
-          if ((++i & 63) == 0 && batch_ns() - t0 > 2000000000ull) {
+          if (((++i & 63) == 0 && batch_ns() - t0 > g.wait_ns) || i >= kBatchMaxPolls) {
             atomicOr(err, 2);
             ok = 0;
             break;
@@ -168,7 +174,7 @@ __global__ void __launch_bounds__(kBatchStreamThreads)
     if (lane == 0) {
       ok = *(volatile int*)err == 0;
       if (ok && w.y > 0) {
-        const int need = g.ntx * g.nty;
+        const int need = g.ntx * g.nty + g.hold;
         volatile int* c = counters + g.cnt_off + w.y - 1;
         const uint64_t t0 = batch_ns();
         unsigned i = 0;
@@ -177,7 +183,7 @@ __global__ void __launch_bounds__(kBatchStreamThreads)
             ok = 0;
             break;
           }
-          if ((++i & 63) == 0 && batch_ns() - t0 > 2000000000ull) {
+          if (((++i & 63) == 0 && batch_ns() - t0 > g.wait_ns) || i >= kBatchMaxPolls) {
             atomicOr(err, 2);
             ok = 0;
             break;
@@ -385,6 +391,8 @@ ots_status ots_batch_create(const ots_params* grids, int32_t n, int32_t device, 
     g.op_args.coef = g.op == 0 ? (p.coef != 0.0f ? p.coef : 1.0f / 5.0f) : p.coef;
     const double h = g.n > 1 ? 1.0 / (double)(g.n - 1) : 1.0;
     g.op_args.h2 = p.h2 != 0.0f ? p.h2 : (float)(h * h);
+    g.wait_ns = ots::kBatchWaitNs;
+    g.hold = 0;
     off[i] = floats;
     floats += (size_t)(g.op == 1 ? 3 : 2) * g.sy * g.n;
     b->updates += (int64_t)g.n * g.n * g.steps;
@@ -482,6 +490,30 @@ ots_status ots_batch_create(const ots_params* grids, int32_t n, int32_t device, 
 }
 
 void ots_batch_destroy(ots_batch* b) { free_batch(b); }
+
+static ots_status upload_grids(ots_batch* b) {
+  B_CUDA(cudaSetDevice(b->device), "cudaSetDevice");
+  B_CUDA(cudaStreamSynchronize(b->stream), "synchronize");
+  B_CUDA(cudaMemcpy(b->d_grids, b->grids.data(), b->ngrids * sizeof(ots::BatchGrid),
+                    cudaMemcpyHostToDevice),
+         "grid table upload");
+  return OTS_OK;
+}
+
+ots_status ots_batch_set_wait_limit(ots_batch* b, double seconds) {
+  if (!b) return bfail(OTS_ERR_INVALID_ARGUMENT, "batch is NULL");
+  if (!(seconds > 0.0 && seconds <= 60.0))
+    return bfail(OTS_ERR_INVALID_ARGUMENT, "wait limit must be in (0, 60] seconds");
+  for (auto& g : b->grids) g.wait_ns = (uint64_t)(seconds * 1e9);
+  return upload_grids(b);
+}
+
+ots_status ots_batch_debug_hold(ots_batch* b, int32_t grid) {
+  if (!b) return bfail(OTS_ERR_INVALID_ARGUMENT, "batch is NULL");
+  if (grid >= b->ngrids) return bfail(OTS_ERR_INVALID_ARGUMENT, "bad grid index");
+  for (int i = 0; i < b->ngrids; ++i) b->grids[i].hold = (i == grid) ? 1 : 0;
+  return upload_grids(b);
+}
 
 ots_status ots_batch_info(const ots_batch* b, int64_t* updates, int32_t* items, int32_t* ctas) {
   if (!b) return bfail(OTS_ERR_INVALID_ARGUMENT, "batch is NULL");

@@ -92,6 +92,15 @@ __global__ void k_silu(const float* __restrict__ Z, float* __restrict__ A, int n
   if (i < n) A[i] = Z[i] * sigmoid(Z[i]);
 }
 
+// In place: A = silu(A) (one pointer, no aliasing promise).
+__global__ void k_silu_inplace(float* A, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    const float z = A[i];
+    A[i] = z * sigmoid(z);
+  }
+}
+
 // dZ = dA * silu'(Z), silu'(z) = s(z) (1 + z (1 - s(z)))
 __global__ void k_silu_bwd(const float* __restrict__ dA, const float* __restrict__ Z,
                            float* __restrict__ dZ, int n) {
@@ -616,7 +625,7 @@ ots_status ots_mlp_predict_noalloc(const ots_mlp* m, const float* X, int32_t n, 
     gemm(s, n, O, I, buf[cur], I, 0, m->d_params + m->w_off[l], I, 1, buf[cur ^ 1], O,
          m->d_params + m->b_off[l]);
     if (l < m->layers - 1)
-      k_silu<<<cdiv(n * O, 256), 256, 0, s>>>(buf[cur ^ 1], buf[cur ^ 1], n * O);
+      k_silu_inplace<<<cdiv(n * O, 256), 256, 0, s>>>(buf[cur ^ 1], n * O);
     cur ^= 1;
   }
   k_affine<<<cdiv(n, 256), 256, 0, s>>>(buf[cur], y, n, m->y_std, m->y_mean);

@@ -209,6 +209,8 @@ struct ots_plan {
   float* aux[2] = {};
   int cur = 0;
   int* d_err = nullptr;
+  uint64_t wait_ns = ots::kWaitNs;  // limit of the stream kernel's bounded waits
+  int hold_plane = -1;              // test hook (ots_plan_debug_hold_plane)
   // -c clock recording (tile kernel): kClockWords per warp of the last launch
   unsigned* d_clocks = nullptr;
   int64_t clock_warps = 0;
@@ -822,6 +824,8 @@ ots_status enqueue_run(ots_plan* pl, int kernel) {
       sp.cy = c.cy;
       sp.base_step = base;
       sp.err = pl->d_err;
+      sp.wait_ns = pl->wait_ns;
+      sp.hold_plane = pl->hold_plane;
       sp.op = pl->op;
       CUtensorMap m;
       if (Tl == pl->scfg.T) {
@@ -1391,6 +1395,20 @@ ots_status ots_plan_device_aux(const ots_plan* plan, int32_t field, float** ptr)
   if (!plan || !ptr || field < 0 || field >= plan->info->na)
     return fail(OTS_ERR_INVALID_ARGUMENT, "bad aux field request");
   *ptr = plan->aux[field];
+  return OTS_OK;
+}
+
+ots_status ots_plan_set_wait_limit(ots_plan* pl, double seconds) {
+  if (!pl) return fail(OTS_ERR_INVALID_ARGUMENT, "NULL plan");
+  if (!(seconds > 0.0 && seconds <= 60.0))
+    return fail(OTS_ERR_INVALID_ARGUMENT, "wait limit must be in (0, 60] seconds");
+  pl->wait_ns = (uint64_t)(seconds * 1e9);
+  return OTS_OK;
+}
+
+ots_status ots_plan_debug_hold_plane(ots_plan* pl, int32_t plane) {
+  if (!pl) return fail(OTS_ERR_INVALID_ARGUMENT, "NULL plan");
+  pl->hold_plane = plane < 0 ? -1 : plane;
   return OTS_OK;
 }
 

@@ -23,8 +23,10 @@
 //     of T + 2 planes, one plane ahead of its first use, so every level reads
 //     its plane's f from shared memory.
 //
-// Every mbarrier wait is bounded; on timeout the CTA records an error word
-// and all its threads leave together (the host reports OTS_ERR_TIMEOUT).
+// Every mbarrier wait is bounded (p.wait_ns, 2 s unless the host sets it);
+// on timeout the CTA records an error word, waits (bounded by time only)
+// for its own copies still in flight, and all its threads leave together
+// (the host reports OTS_ERR_TIMEOUT).
 #pragma once
 
 #include <cuda.h>
@@ -47,6 +49,8 @@ struct StreamParams {
   int cy;            // CTAs per cluster along y (grid mode); 0 or 1 = no cluster
   int base_step;     // global step index of this launch's first level
   int* err;          // device error word (bit 0: mbarrier wait timed out)
+  uint64_t wait_ns;  // limit of every bounded wait (default kWaitNs)
+  int hold_plane;    // test hook: CTA 0 never loads this running plane (-1: off)
   OpArgs op;
 };
 
@@ -55,7 +59,7 @@ struct StreamParams {
 #endif
 constexpr int kStreamStages = OTS_STREAM_STAGES;  // ring depth (power of 2); lookahead = stages - 2
 constexpr unsigned kWaitLimit = 1u << 24;
-constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s
+constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s: default limit of a bounded wait
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -88,19 +92,34 @@ __device__ __forceinline__ uint64_t global_ns() {
   return t;
 }
 
-// Bounded wait: false if the phase did not complete within kWaitNs of wall
-// time, within kWaitLimit polls, or once another CTA has raised the error
-// word (then every CTA stops waiting soon after the first failure).
+// Bounded wait: false if the phase did not complete within `limit_ns` of
+// wall time, within kWaitLimit polls, or once another CTA has raised the
+// error word (then every CTA stops waiting soon after the first failure).
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity,
-                                                  const int* err) {
+                                                  const int* err, uint64_t limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_ns();
   for (unsigned i = 0; i < kWaitLimit; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
     if ((i & 255) == 255) {
-      if (global_ns() - t0 > kWaitNs) return false;
+      if (global_ns() - t0 > limit_ns) return false;
       if (*(volatile const int*)err != 0) return false;
     }
+  }
+  return false;
+}
+
+// Drain wait of a failing CTA for one of its own copies still in flight:
+// bounded by time and polls only, never cut short by the error word (the
+// CTA raised it itself), so the CTA leaves only once the copy has landed or
+// the limit has passed.
+__device__ __forceinline__ bool mbar_wait_drain(uint64_t* bar, unsigned parity,
+                                                uint64_t limit_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (unsigned i = 0; i < kWaitLimit; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 255) == 255 && global_ns() - t0 > limit_ns) return false;
   }
   return false;
 }
@@ -342,11 +361,15 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
 
   // every thread is past the previous segment's reads of the ring
   __syncthreads();
+  // test hook: CTA 0 arms the stage of running plane hold_plane but never
+  // loads it, so that plane's wait can only run out (a flag nothing sets)
+  const bool hold_cta = p.hold_plane >= 0 && blockIdx.x == 0 && blockIdx.y == 0;
   if (tid == 0) {
     for (int j = 0; j < LA && j < nit; ++j) {
       const int g = rg + j;
       mbar_arrive_expect_tx(&bars[g & (NST - 1)], box_bytes);
-      tma_load_3d(smem + (g & (NST - 1)) * PL, &tmap, tx0, ty0, kb + j, &bars[g & (NST - 1)]);
+      if (!(hold_cta && g == p.hold_plane))
+        tma_load_3d(smem + (g & (NST - 1)) * PL, &tmap, tx0, ty0, kb + j, &bars[g & (NST - 1)]);
     }
     if (FR && nit > 1) {  // f of plane kb, first read at iteration 1
       const int fs = rg % (NF > 0 ? NF : 1);
@@ -361,10 +384,10 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
     const int k = kb + r;
     const int g = rg + r;  // running plane index: ring stage and phase parity
     const int st = g & (NST - 1);
-    bool to = !mbar_wait_bounded(&bars[st], (g / NST) & 1, p.err);
+    bool to = !mbar_wait_bounded(&bars[st], (g / NST) & 1, p.err, p.wait_ns);
     if (FR && r >= 1 && !to)  // f of plane k - 1, first read by level 1 now
       to = !mbar_wait_bounded(&fbars[(g - 1) % (NF > 0 ? NF : 1)],
-                              ((g - 1) / (NF > 0 ? NF : 1)) & 1, p.err);
+                              ((g - 1) / (NF > 0 ? NF : 1)) & 1, p.err, p.wait_ns);
     // cluster halo: the neighbours' rows of plane r-1 (slot of phase hg+r-1)
     const int hr = (hg + r + kHaloSlots - 1) % kHaloSlots;
     const unsigned hpar = (unsigned)((hg + r - 1) / kHaloSlots) & 1u;
@@ -388,7 +411,8 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
     if (tid == 0 && r + LA < nit) {
       const int s2 = (g + LA) & (NST - 1);
       mbar_arrive_expect_tx(&bars[s2], box_bytes);
-      tma_load_3d(smem + s2 * PL, &tmap, tx0, ty0, k + LA, &bars[s2]);
+      if (!(hold_cta && g + LA == p.hold_plane))
+        tma_load_3d(smem + s2 * PL, &tmap, tx0, ty0, k + LA, &bars[s2]);
     }
     // f of plane k + 1 (read from iteration r + 2 on) into the slot of plane
     // k + 1 - NF = k - T - 1, whose last reader was level T one iteration ago
@@ -419,9 +443,10 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
       const int q = k - t;
       const int cp = (t == 1) ? pc0 : xr + (t - 2) * 2 * PL;
       if (r > 0 && !lost) {  // neighbour rows of level t-1, plane r-1
-        if (top_ext) lost = !mbar_wait_bounded(&hbars[(hr * T + t - 1) * 2 + 0], hpar, p.err);
+        if (top_ext)
+          lost = !mbar_wait_bounded(&hbars[(hr * T + t - 1) * 2 + 0], hpar, p.err, p.wait_ns);
         if (bot_ext && !lost)
-          lost = !mbar_wait_bounded(&hbars[(hr * T + t - 1) * 2 + 1], hpar, p.err);
+          lost = !mbar_wait_bounded(&hbars[(hr * T + t - 1) * 2 + 1], hpar, p.err, p.wait_ns);
       }
       const float* const tp = top_ext ? hrow + (t - 1) * 2 * TX : smem + cp + o_top;
       const float* const bp = bot_ext ? hrow + (t - 1) * 2 * TX + TX : smem + cp + o_bot;
@@ -561,15 +586,18 @@ __global__ void __launch_bounds__(StreamThreads<T, E>::kMax, 1)
   if (!ok) {
     if (tid == 0) {
       atomicOr(p.err, 1);
-      // drain this CTA's copies still in flight (bounded) before leaving:
-      // running planes fail_r .. fail_r + LA - 1 were issued
+      // drain this CTA's copies still in flight before leaving, each wait
+      // bounded by time only: running planes fail_r .. fail_r + LA - 1 were
+      // issued
       for (int j = fail_r; j < rg + nit && j < fail_r + LA; ++j)
-        mbar_wait_bounded(&bars[j & (NST - 1)], (j / NST) & 1, p.err);
+        mbar_wait_drain(&bars[j & (NST - 1)], (j / NST) & 1, p.wait_ns);
       // aux planes issued but not yet waited for: up to the failing iteration's
       // own plane (issued one iteration before it), from its k - 1 on
       if (FR)
         for (int j = fail_r - 1; j <= fail_r && j < rg + nit - 1; ++j)
-          if (j >= rg) mbar_wait_bounded(&fbars[j % (NF > 0 ? NF : 1)], (j / (NF > 0 ? NF : 1)) & 1, p.err);
+          if (j >= rg)
+            mbar_wait_drain(&fbars[j % (NF > 0 ? NF : 1)], (j / (NF > 0 ? NF : 1)) & 1,
+                            p.wait_ns);
     }
     __syncthreads();
   }

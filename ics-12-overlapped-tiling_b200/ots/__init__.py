@@ -154,6 +154,10 @@ def lib():
     L.ots_plan_clock_records.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
                                          ctypes.POINTER(ctypes.c_int64)]
     L.ots_plan_clock_records.restype = st
+    L.ots_plan_set_wait_limit.argtypes = [ctypes.c_void_p, ctypes.c_double]
+    L.ots_plan_set_wait_limit.restype = st
+    L.ots_plan_debug_hold_plane.argtypes = [ctypes.c_void_p, ctypes.c_int32]
+    L.ots_plan_debug_hold_plane.restype = st
     L.ots_host_register.argtypes = [ctypes.c_void_p, ctypes.c_size_t]
     L.ots_host_register.restype = st
     L.ots_host_unregister.argtypes = [ctypes.c_void_p]
@@ -401,6 +405,15 @@ class Plan:
             check(lib().ots_plan_clock_records(self.handle, out.ctypes.data, n.value,
                                                ctypes.byref(n)))
         return out
+
+    def set_wait_limit(self, seconds):
+        """Limit of the 3D stream kernel's bounded device waits (2 s default)."""
+        check(lib().ots_plan_set_wait_limit(self.handle, float(seconds)))
+
+    def debug_hold_plane(self, plane):
+        """Test hook: the first CTA never loads this running plane, so its
+        wait runs out (the run reports TIMEOUT); -1 turns it off."""
+        check(lib().ots_plan_debug_hold_plane(self.handle, int(plane)))
 
     def stream_ptr(self):
         p = ctypes.c_void_p()

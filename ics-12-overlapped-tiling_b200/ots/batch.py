@@ -51,6 +51,10 @@ def _blib():
         L.ots_batch_stream.restype = ctypes.c_int
         L.ots_batch_run_sequential.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(Timing)]
         L.ots_batch_run_sequential.restype = ctypes.c_int
+        L.ots_batch_set_wait_limit.argtypes = [vp, ctypes.c_double]
+        L.ots_batch_set_wait_limit.restype = ctypes.c_int
+        L.ots_batch_debug_hold.argtypes = [vp, ctypes.c_int32]
+        L.ots_batch_debug_hold.restype = ctypes.c_int
         L._batch_ready = True
     return L
 
@@ -153,6 +157,14 @@ class Batch:
         t = Timing()
         check(_blib().ots_batch_run(self.h, ctypes.byref(t)))
         return t.event_ms * 1e-3
+
+    def set_wait_limit(self, seconds):
+        """Limit of each item's bounded wait for its grid's previous chunk."""
+        check(_blib().ots_batch_set_wait_limit(self.h, float(seconds)))
+
+    def debug_hold(self, grid):
+        """Test hook: grid's later chunks wait for a count never reached (-1: off)."""
+        check(_blib().ots_batch_debug_hold(self.h, int(grid)))
 
     def run_sequential(self, kernel="plain"):
         t = Timing()

@@ -288,6 +288,16 @@ ots_status ots_plan_enable_clocks(ots_plan* plan, int32_t enable);
 ots_status ots_plan_clock_records(ots_plan* plan, ots_clock_record* out, int64_t capacity,
                                   int64_t* count);
 
+/* Limit of every bounded device wait of the plan's 3D stream kernel (its
+ * TMA ring barriers), 2 s by default; a wait that runs out makes the run
+ * return OTS_ERR_TIMEOUT and leaves the context usable.  No reference
+ * counterpart (the reference's in-order OpenCL queue has no device waits). */
+ots_status ots_plan_set_wait_limit(ots_plan* plan, double seconds);
+/* Test hook, no reference counterpart: with plane >= 0 the first CTA of the
+ * 3D stream kernel arms the ring barrier of that running plane but never
+ * loads it, so its wait runs out (OTS_ERR_TIMEOUT); -1 turns it off. */
+ots_status ots_plan_debug_hold_plane(ots_plan* plan, int32_t plane);
+
 /* Page-lock a caller's host buffer so uploads/downloads run as async DMA. */
 ots_status ots_host_register(void* ptr, size_t bytes);
 ots_status ots_host_unregister(void* ptr);
@@ -315,6 +325,13 @@ ots_status ots_batch_download(ots_batch* batch, int32_t grid, float* state);
 ots_status ots_batch_run(ots_batch* batch, ots_timing* timing);
 ots_status ots_batch_run_async(ots_batch* batch);
 ots_status ots_batch_stream(const ots_batch* batch, void** cuda_stream);
+/* Limit of each item's bounded wait for its grid's previous chunk (2 s by
+ * default); a wait that runs out makes ots_batch_run return
+ * OTS_ERR_TIMEOUT.  Test hook: ots_batch_debug_hold(batch, g) makes every
+ * later chunk of grid g wait for a completion count that is never reached
+ * (-1 releases it).  No reference counterpart. */
+ots_status ots_batch_set_wait_limit(ots_batch* batch, double seconds);
+ots_status ots_batch_debug_hold(ots_batch* batch, int32_t grid);
 /* Comparator on the same buffers: the grids one after another with one
  * launch per step (OTS_KERNEL_PLAIN) or per T steps (OTS_KERNEL_TILE). */
 ots_status ots_batch_run_sequential(ots_batch* batch, int32_t kernel, ots_timing* timing);
@@ -352,9 +369,10 @@ ots_status ots_mlp_topk(ots_mlp* model, const float* X, int32_t n, int32_t k, in
 
 /* Cost-model inference that allocates nothing -- no counterpart in the
  * reference.  For callers that must not call cudaMalloc while they pick
- * configurations: an application that owns all device memory through its own
- * pool, or one that is capturing work into a CUDA graph (cudaMalloc cannot be
- * captured).  X (n x n_in, row-major) and y (n) are DEVICE pointers the caller
+ * configurations: an application that hands out all device memory from its
+ * own pool and does not let libraries allocate behind its back, or code that
+ * runs where an allocation could block or fail at the wrong moment.  X
+ * (n x n_in, row-major) and y (n) are DEVICE pointers the caller
  * owns; the work is enqueued on `cuda_stream` (a cudaStream_t, NULL for the
  * default stream) and this call does not wait for it.
  *   - The activations live in one fixed 2 MiB array compiled into libots

@@ -134,3 +134,32 @@ def test_read_dat_reference_layout(tmp_path):
     rows = A.read_dat(str(p))
     assert rows == [{"Block Size X": "32", "EventElapsed": "0.5"},
                     {"Block Size X": "64", "EventElapsed": "0.25"}]
+
+
+def test_watchdog_skips_a_hung_run_and_the_sweep_continues(tmp_path):
+    """scripts/utils.py:134-145: a run that outlives the watchdog is killed,
+    reported as a failure and left out of the raw file; the next runs go on.
+    The runner is a fake script that hangs (sleeps) for block size 64 only."""
+    runner = tmp_path / "fake-runner"
+    runner.write_text(
+        "#!/bin/sh\n"
+        "bx=0\n"
+        "while [ $# -gt 0 ]; do [ \"$1\" = -x ] && bx=$2; shift; done\n"
+        "if [ \"$bx\" = 64 ]; then exec sleep 30; fi\n"
+        "echo \"Block Size X: $bx\"\n"
+        "echo \"EventElapsed: 0.5\"\n")
+    runner.chmod(0o755)
+    y = tmp_path / "exp.yml"
+    y.write_text("name: wd\noutfile: wd.raw.dat\nbinary: fake-runner\ndimensions: 2\n"
+                 "parameters:\n  block_size_x: [32, 96, 32]\n  problem_size: 64\n")
+    logs = []
+    t0 = __import__("time").time()
+    ok, failed = H.run_experiment(str(y), watchdog=1.0, log=logs.append)
+    assert __import__("time").time() - t0 < 20
+    assert (ok, failed) == (2, 1)
+    assert "Watchdog timer expired!" in logs
+    assert logs.index("Watchdog timer expired!") > logs.index("Running 2 of 3")
+    assert "Running 3 of 3" in logs  # the sweep went on past the hung run
+    raw = (tmp_path / "wd.raw.dat").read_text().splitlines()
+    assert raw == ["1#Block Size X: 32", "1#EventElapsed: 0.5",
+                   "3#Block Size X: 96", "3#EventElapsed: 0.5"]

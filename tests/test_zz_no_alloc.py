@@ -2,8 +2,8 @@
 
 Some callers of the configuration picker cannot call cudaMalloc at the
 moment they ask for a prediction -- an application that hands out all device
-memory from its own pool, or one that is capturing its work into a CUDA graph
-(cudaMalloc cannot be captured).  ots_mlp_predict_noalloc serves them from a
+memory from its own pool and lets no library allocate behind its back.
+ots_mlp_predict_noalloc serves them from a
 fixed 2 MiB array compiled into libots: the caller passes device input and
 output buffers and a stream, and the call allocates nothing.
 
