@@ -390,23 +390,33 @@ struct OpGradient3D {
 };
 
 // opencl/cs-3d/cs-3d.cpp:161-163 constants, :284-308 arithmetic with y+1 as
-// the "p1" direction throughout (the reference's step-1 code flips it).
+// the "p1" direction throughout (the reference's step-1 code flips its two
+// y-axis neighbours).  The generated text #defines eps as (1e-9), a double
+// literal (:161), which makes each c term a double expression: the float
+// squares are summed onto 1e-9 in double, 1/sqrt, multiplied by u and
+// divided by 1.1f in double, and rounded to float once.  Double sqrt and
+// division are IEEE on both the GPU and the host, so this stencil matches the
+// CPU oracle bit for bit.
 struct OpCs3D {
   static constexpr int DIMS = 3, NS = 1, NA = 0, RX = 1, RY = 1, RZ = 1;
   static constexpr bool STAR = false;
+  OTS_HD static float cterm(float u, float a, float b, float c) {
+    return (float)((double)u * (1.0 / sqrt(1e-9 + (double)a + (double)b + (double)c)) /
+                   (double)1.1f);
+  }
   template <class A>
   OTS_HD static void apply(const A& a, const float*, const OpArgs&, int,
                                                float* o) {
-    const float EPS = 1e-9f, SUMAREF = 1.1f, ALPHA = 1.1f;
+    const float ALPHA = 1.1f;
     float u = a(0, 0, 0, 0);
     float zp = a(0, 1, 0, 0), zm = a(0, -1, 0, 0), yp = a(0, 0, 1, 0), ym = a(0, 0, -1, 0),
           xp = a(0, 0, 0, 1), xm = a(0, 0, 0, -1);
     float zm_yp = a(0, -1, 1, 0), zm_xp = a(0, -1, 0, 1), zp_ym = a(0, 1, -1, 0),
           ym_xp = a(0, 0, -1, 1), zp_xm = a(0, 1, 0, -1), yp_xm = a(0, 0, 1, -1);
-    float c1 = u * ots_rsqrt(EPS + sq(zp - u) + sq(yp - u) + sq(xp - u)) / SUMAREF;
-    float c2 = u * ots_rsqrt(EPS + sq(u - zm) + sq(zm_yp - zm) + sq(zm_xp - zm)) / SUMAREF;
-    float c3 = u * ots_rsqrt(EPS + sq(zp_ym - ym) + sq(u - ym) + sq(ym_xp - ym)) / SUMAREF;
-    float c4 = u * ots_rsqrt(EPS + sq(zp_xm - xm) + sq(yp_xm - xm) + sq(u - xm)) / SUMAREF;
+    float c1 = cterm(u, sq(zp - u), sq(yp - u), sq(xp - u));
+    float c2 = cterm(u, sq(u - zm), sq(zm_yp - zm), sq(zm_xp - zm));
+    float c3 = cterm(u, sq(zp_ym - ym), sq(u - ym), sq(ym_xp - ym));
+    float c4 = cterm(u, sq(zp_xm - xm), sq(yp_xm - xm), sq(u - xm));
     o[0] = (ALPHA * u + c1 * (zp + yp + xp) + c2 * zm + c3 * ym + c4 * xm) /
            (ALPHA + 3.0f * c1 + c2 + c3 + c4);
   }

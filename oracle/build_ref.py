@@ -128,6 +128,112 @@ def gen_geometry_and_fill(ref_root):
         fh.write("".join(out))
 
 
+# Generated-kernel pins: name -> (runner source, generator class, stencil id
+# in the oracle's numbering).  These seven runners have no usable CPU check
+# (Jacobi copies, a commented-out one, or jacobi-3d's out-of-bounds loop), so
+# the oracle is pinned to the kernels their own generators emit.
+GENERATORS = {
+    "jacobi_3d": ("opencl/jacobi-3d/jacobi-3d.cpp", "Jacobi3DGenerator", 4),
+    "poisson_3d": ("opencl/poisson-3d/poisson-3d.cpp", "Poisson3DGenerator", 6),
+    "gradient_3d": ("opencl/gradient-3d/gradient-3d.cpp", "Gradient3DGenerator", 8),
+    "fdtd_2d": ("opencl/fdtd-2d/fdtd-2d.cpp", "FDTD2DGenerator", 9),
+    "rician_denoise_2d": ("opencl/rician-denoise-2d/rician-denoise-2d.cpp",
+                          "Rician2DGenerator", 10),
+    "cdsc_tv_update_2d": ("opencl/cdsc-tv-update-2d/cdsc-tv-update-2d.cpp",
+                          "TVUpdate2DGenerator", 11),
+    "cs_3d": ("opencl/cs-3d/cs-3d.cpp", "CS3DGenerator", 12),
+}
+GEN_LIB = os.path.join(OUT, "libots_refgen.so")
+
+
+def gen_generators(ref_root, cxx="g++"):
+    """oracle/_ref/ref_generators.cpp -> libots_refgen.so: each runner's
+    GeneratorParams and XGenerator (its source from ``struct GeneratorParams``
+    up to ``compareResults``, copied verbatim into its own namespace) behind
+    ``extern "C" int gen_<name>(n, T, bx, by, bz, E, steps, buf, cap)``,
+    which fills ``buf`` with the kernel text generate() returns (-1 if
+    computeDerived throws, -2 if the text does not fit)."""
+    out = ['#include <cstring>\n#include <iostream>\n#include <sstream>\n#include <string>\n',
+           '#include "ref_shim.hpp"\n',
+           # printProgramParameters (never called here) names printValue
+           "template <class V> void printValue(const std::string&, const V&) {}\n",
+           '#include "ProgramGenerator.hpp"\n',
+           "namespace ot {\nProgramGenerator::ProgramGenerator() {}\n"
+           "ProgramGenerator::~ProgramGenerator() {}\n"
+           "std::string ProgramGenerator::getProgram() { return std::string(); }\n}\n"]
+    for name, (rel, cls, _) in GENERATORS.items():
+        path = os.path.join(ref_root, rel)
+        line, body = extract_between(path, lambda l: l.startswith("struct GeneratorParams"),
+                                     lambda l: l.startswith("void compareResults("))
+        body = body[:body.rindex("void compareResults(")]
+        out.append("namespace refgen_%s {\nusing namespace ot;\n#line %d \"%s\"\n%s\n}\n"
+                   % (name, line, path, body))
+        out.append(
+            'extern "C" int gen_%s(int n, int T, int bx, int by, int bz, int E, int steps,\n'
+            "                      char* buf, int cap) {\n"
+            "  std::string text;\n"
+            "  try {\n"
+            "    refgen_%s::GeneratorParams p;\n"
+            "    p.problemSize = n; p.timeTileSize = T; p.timeSteps = steps;\n"
+            "    p.blockSizeX = bx; p.blockSizeY = by; p.blockSizeZ = bz;\n"
+            "    p.elementsPerThread = E;\n"
+            "    refgen_%s::%s g;\n"
+            "    text = g.generate(p);\n"
+            "  } catch (...) { return -1; }\n"
+            "  if ((int)text.size() + 1 > cap) return -2;\n"
+            "  std::memcpy(buf, text.c_str(), text.size() + 1);\n"
+            "  return (int)text.size();\n}\n" % (name, name, name, cls))
+    src = os.path.join(OUT, "ref_generators.cpp")
+    with open(src, "w") as fh:
+        fh.write("".join(out))
+    inc = os.path.join(ref_root, "opencl", "common", "inc")
+    subprocess.check_call([cxx, "-O1", "-fPIC", "-shared", "-w", "-I", HERE, "-I", inc, src,
+                           "-o", GEN_LIB])
+
+
+def kernel_text(stencil, n, T, bx, by, bz, E, steps):
+    """The kernel source the reference's generator emits for one case (needs
+    libots_refgen.so, built by build())."""
+    import ctypes
+    lib = ctypes.CDLL(GEN_LIB)
+    fn = getattr(lib, "gen_" + stencil.replace("-", "_"))
+    fn.argtypes = [ctypes.c_int] * 7 + [ctypes.c_char_p, ctypes.c_int]
+    buf = ctypes.create_string_buffer(1 << 22)
+    rc = fn(n, T, bx, by, bz, E, steps, buf, len(buf))
+    if rc < 0:
+        raise ValueError("reference generator refused %s n=%d T=%d %dx%dx%d E=%d (rc %d)"
+                         % (stencil, n, T, bx, by, bz, E, rc))
+    return buf.value.decode()
+
+
+# Rician's phase 2 stores the new value into bufferU while neighbouring
+# work-items still read bufferU in the same phase (a race,
+# opencl/rician-denoise-2d/rician-denoise-2d.cpp:322-329).  At T = 1 nothing
+# reads that store (the write-back takes local0), so the case drops it.
+RICIAN_T1_DEAD_STORE = "    bufferU[get_local_id(1)*1+0+1][get_local_id(0)+1] = local0;\n"
+
+
+def build_kernel_case(stencil, n, T, bx, by, bz, E, steps, cxx="g++"):
+    """Emit one case's kernel text with the reference's generator and compile
+    oracle/ref_clkernel.cpp around it; returns the shared library's path."""
+    text = kernel_text(stencil, n, T, bx, by, bz, E, steps)
+    if stencil == "rician-denoise-2d":
+        if T != 1 or E != 1 or text.count(RICIAN_T1_DEAD_STORE) != 1:
+            raise ValueError("rician pin cases are T = 1, E = 1 only")
+        text = text.replace(RICIAN_T1_DEAD_STORE, "")
+    tag = "%s_n%d_T%d_%dx%dx%d_E%d_s%d" % (stencil.replace("-", "_"), n, T, bx, by, bz, E, steps)
+    cl = os.path.join(OUT, "clk_%s.cl" % tag)
+    with open(cl, "w") as fh:
+        fh.write(text)
+    lib = os.path.join(OUT, "libclk_%s.so" % tag)
+    sid = GENERATORS[stencil.replace("-", "_")][2]
+    subprocess.check_call([cxx, "-std=c++20", "-O1", "-ffp-contract=off", "-fPIC", "-shared",
+                           "-pthread", "-w", '-DOTS_CL_KERNEL_FILE="%s"' % cl,
+                           "-DOTS_CL_STENCIL=%d" % sid, os.path.join(HERE, "ref_clkernel.cpp"),
+                           "-o", lib])
+    return lib
+
+
 def build(ref_root=None, cxx="g++", verbose=False):
     ref_root = ref_root or os.environ.get("OTS_REFERENCE_DIR", "/root/reference")
     if not os.path.isdir(os.path.join(ref_root, "opencl")):
@@ -141,6 +247,7 @@ def build(ref_root=None, cxx="g++", verbose=False):
             fh.write('#line %d "%s"\n' % (line, path))
             fh.write(body)
     gen_geometry_and_fill(ref_root)
+    gen_generators(ref_root, cxx)
     lib = os.path.join(OUT, "libots_ref.so")
     cmd = [cxx, "-O2", "-g", "-fPIC", "-shared", "-I", OUT, "-I", HERE,
            os.path.join(HERE, "ref_harness.cpp"), os.path.join(OUT, "ref_gen.cpp"), "-o", lib]

@@ -228,3 +228,23 @@ def ref_fill(which, P, padding, seed):
     fn.argtypes = [_F] * nf + [ctypes.c_int, ctypes.c_int, ctypes.c_uint]
     fn(*[_fp(a) for a in arrs], P, padding, seed)
     return arrs
+
+
+def ref_kernel_run(lib_path, fields, aux=(), T=1, steps=1, nb=(1, 1, 1), bs=(1, 1, 1)):
+    """Run a reference-generated kernel compiled for the CPU by
+    build_ref.build_kernel_case (the runner's launch loop over copies of
+    `fields`, aux read-only in the runner's argument order); returns the
+    final fields."""
+    lib = ctypes.CDLL(lib_path)
+    fn = lib.clk_run
+    fn.argtypes = [ctypes.POINTER(_F), ctypes.POINTER(_F), ctypes.c_int, ctypes.c_int,
+                   ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                   ctypes.POINTER(ctypes.c_int)]
+    st = [np.ascontiguousarray(f, np.float32).copy() for f in fields]
+    ax = [np.ascontiguousarray(a, np.float32) for a in aux]
+    sp = (_F * len(st))(*[_fp(a) for a in st])
+    apn = (_F * max(1, len(ax)))(*[_fp(a) for a in ax])
+    nbc = (ctypes.c_int * 3)(*nb)
+    bsc = (ctypes.c_int * 3)(*bs)
+    fn(sp, apn, len(st), st[0].shape[0], st[0].ndim, T, steps, nbc, bsc)
+    return st

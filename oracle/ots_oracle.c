@@ -102,7 +102,6 @@ static void orc_par_copy(void* dst, const void* src, size_t bytes, int nth) {
 #define TV_EPI1  1e-8f
 #define TV_ALPHA 1.1f
 /* opencl/cs-3d/cs-3d.cpp:161-163 */
-#define CS_EPS     1e-9f
 #define CS_SUMAREF 1.1f
 #define CS_ALPHA   1.1f
 

@@ -12,6 +12,14 @@ Outputs:
   ref_loops.npz     inputs and outputs of the reference CPU loops
   ref_fills.npz     outputs of the reference fill loops
   ref_geometry.json computeDerived results for a seeded sample of parameters
+  ref_kernels.npz   inputs and outputs of the kernels the reference's own
+                    generators emit (XGenerator::generate), run on the CPU by
+                    oracle/ref_clkernel.cpp, for the seven stencils whose
+                    runners have no usable CPU check
+
+    python tests/golden/make_golden.py [loops] [fills] [geometry] [kernels]
+
+writes the named fixtures (all four without arguments).
 """
 import json
 import os
@@ -95,10 +103,70 @@ def geometry():
         json.dump(rows, fh, separators=(",", ":"))
 
 
+# Generated-kernel cases: (stencil, n, T, bx, by, bz, E, steps, seed, oracle variant).
+# Constraints that keep each case clear of the reference kernels' known
+# defects (SURVEY Appendix A is not needed to read them; each is stated):
+#   * 3D: bx == bz, so the local array declared [sZ][sY][sZ] has the shape
+#     the kernel indexes ([sZ][sY][sX], opencl/jacobi-3d/jacobi-3d.cpp:189-190);
+#   * 3D at T = 2: one tile along z (n == bz - 2), so the write-back that
+#     ignores writeValidZ (:400-405) writes only the zero ring's planes;
+#   * fdtd-2d and rician at T = 1: one tile covering the interior -- their
+#     second phase reads E' / g of the cells right of and below the tile,
+#     which no work-item of the tile computes; with one tile those cells are
+#     the zero ring and read as zero;
+#   * cs-3d: variant 2, the first step's y-axis orientation (cs-3d.cpp:259-283).
+KERNEL_CASES = [
+    ("jacobi-3d", 16, 1, 4, 4, 4, 1, 5, 123456, 1),
+    ("jacobi-3d", 16, 1, 4, 2, 4, 2, 4, 77, 1),
+    ("jacobi-3d", 6, 2, 8, 4, 8, 1, 6, 123456, 1),
+    ("jacobi-3d", 6, 2, 8, 2, 8, 2, 7, 5, 1),
+    ("poisson-3d", 12, 1, 4, 4, 4, 1, 3, 123456, 1),
+    ("poisson-3d", 6, 2, 8, 4, 8, 1, 4, 9, 1),
+    ("gradient-3d", 12, 1, 4, 4, 4, 1, 4, 123456, 0),
+    ("gradient-3d", 6, 2, 8, 4, 8, 1, 4, 11, 0),
+    ("cs-3d", 12, 1, 4, 4, 4, 1, 4, 123456, 2),
+    ("fdtd-2d", 16, 1, 16, 16, 1, 1, 6, 123456, 1),
+    ("rician-denoise-2d", 16, 1, 16, 16, 1, 1, 4, 123456, 0),
+    ("cdsc-tv-update-2d", 24, 1, 8, 8, 1, 1, 4, 123456, 0),
+]
+
+
+def kernels():
+    """Each case: the reference fill scheme over the runner's interior (every
+    state and aux field, interleaved per cell), the generated kernel run by
+    the runner's launch loop; jacobi-3d's kernel carries its 0.143f weight."""
+    out = {}
+    for k, (st, n, T, bx, by, bz, E, steps, seed, variant) in enumerate(KERNEL_CASES):
+        g = O.ref_geometry(st, n, T, bx, by, bz, E)
+        P, pad, real = g["padded_size"], g["padding"], g["real_size"]
+        d = O.dims(st)
+        nf, na = O.num_state(st), O.num_aux(st)
+        arrs = O.fill_ref(d, P, pad, pad + real, seed, nf + na)
+        fields, aux = arrs[:nf], arrs[nf:]
+        # the runner's argument order: TV takes (input, V, F, ...); the
+        # oracle's aux order is (F, V)
+        ref_aux = aux[::-1] if st == "cdsc-tv-update-2d" else aux
+        nb = [g["num_blocks_x"], g["num_blocks_y"] if d >= 2 else 1,
+              g["num_blocks_z"] if d == 3 else 1]
+        bs = [bx, by if d >= 2 else 1, bz if d == 3 else 1]
+        lib = build_ref.build_kernel_case(st, n, T, bx, by, bz, E, steps)
+        res = O.ref_kernel_run(lib, fields, ref_aux, T=T, steps=steps, nb=nb, bs=bs)
+        key = "k%02d" % k
+        for i, a in enumerate(fields):
+            out["%s_in%d" % (key, i)] = a
+        for i, a in enumerate(aux):
+            out["%s_aux%d" % (key, i)] = a
+        for i, a in enumerate(res):
+            out["%s_out%d" % (key, i)] = a
+        out[key + "_meta"] = np.array([O.SID[st], P, pad, steps, seed, real, T, variant,
+                                       nf, na, bx, by, bz, E], np.int64)
+    np.savez_compressed(os.path.join(HERE, "ref_kernels.npz"), **out)
+
+
 if __name__ == "__main__":
     if not build_ref.build(verbose=True):
         sys.exit("reference tree not found; golden fixtures are generated where it exists")
-    loops()
-    fills()
-    geometry()
-    print("golden fixtures written to", HERE)
+    which = sys.argv[1:] or ["loops", "fills", "geometry", "kernels"]
+    for name in which:
+        {"loops": loops, "fills": fills, "geometry": geometry, "kernels": kernels}[name]()
+    print("golden fixtures written to", HERE, ":", " ".join(which))

@@ -76,3 +76,81 @@ def test_oracle_matches_live_reference_loops(st):
     want = O.ref_loop(st, x, pad, 6)
     got = O.sweep_f32(st, [x], steps=6, lo=pad, hi=P - pad, variant=O.VARIANT_REF)[0]
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def _kernel_cases():
+    p = os.path.join(GOLD, "ref_kernels.npz")
+    z = np.load(p)
+    keys = sorted({k.split("_")[0] for k in z.files})
+    out = []
+    for k in keys:
+        meta = [int(v) for v in z[k + "_meta"]]
+        nf, na = meta[8], meta[9]
+        out.append((k, [z["%s_in%d" % (k, i)] for i in range(nf)],
+                    [z["%s_aux%d" % (k, i)] for i in range(na)],
+                    [z["%s_out%d" % (k, i)] for i in range(nf)], meta))
+    return out
+
+
+@pytest.mark.parametrize("case", _kernel_cases(),
+                         ids=lambda c: "%s-%s-T%d" % (c[0], O.STENCILS[c[4][0]], c[4][6]))
+def test_oracle_matches_reference_generated_kernel(case):
+    """The seven stencils whose runners have no usable CPU check, pinned to
+    the kernels the reference's own generators emit (fixtures made by
+    tests/golden/make_golden.py: the generated OpenCL text run on the CPU by
+    oracle/ref_clkernel.cpp, one thread per work-item, with the runner's
+    launch loop).  Bit for bit: jacobi-3d (weight 0.143f), poisson-3d (26c -
+    the 26 neighbours), gradient-3d, fdtd-2d (the reference's +Ey, no
+    source), rician-denoise-2d, cdsc-tv-update-2d and cs-3d (its first
+    step's y orientation, variant 2), at T = 1 and -- for the 3D star
+    stencils -- through the reference's in-tile time step at T = 2."""
+    key, fields, aux, want, meta = case
+    sid, P, pad, steps, seed, real, T, variant = meta[:8]
+    st = O.STENCILS[sid]
+    coef = float(np.float32(0.143)) if st == "jacobi-3d" else 0.0
+    got = O.sweep_f32(st, fields, aux, steps=steps, lo=pad, hi=pad + real, variant=variant,
+                      coef=coef)
+    for f, (a, b) in enumerate(zip(got, want)):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (
+            st, f, float(np.max(np.abs(a.astype(np.float64) - b))))
+
+
+def test_cs3d_orientation_variants_are_distinct_code_paths():
+    """cs-3d's variant 2 (the reference's first-step y orientation, pinned
+    above) and variant 0 (y+1 as "p1" throughout, the in-tile steps' and the
+    engine's) share every operation but the two y-axis neighbours: they agree
+    where those neighbours are equal and differ on a generic field."""
+    P, pad = 14, 1
+    x = O.fill_ref(3, P, pad, P - pad, 3, 1)[0]
+    c = O.sweep_f32("cs-3d", [x], steps=1, lo=pad, hi=P - pad, variant=0)[0]
+    d = O.sweep_f32("cs-3d", [x], steps=1, lo=pad, hi=P - pad, variant=2)[0]
+    assert not np.array_equal(c, d)
+    # a field constant along y: the y-axis neighbours equal the centre
+    flat = np.ascontiguousarray(np.repeat(x[:, 5:6, :], P, axis=1))
+    flat[:, :pad, :] = 0
+    flat[:, P - pad:, :] = 0
+    e = O.sweep_f32("cs-3d", [flat], steps=1, lo=pad, hi=P - pad, variant=0)[0]
+    f = O.sweep_f32("cs-3d", [flat], steps=1, lo=pad, hi=P - pad, variant=2)[0]
+    inner = (slice(pad, P - pad), slice(pad + 1, P - pad - 1), slice(pad, P - pad))
+    assert np.array_equal(e[inner], f[inner])
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built here")
+def test_generated_kernel_pin_live_on_fresh_inputs():
+    """The same pin run live (where the reference tree is present) on a
+    fresh seed and a case not among the fixtures: jacobi-3d at T = 1 with
+    E = 4 along y."""
+    import build_ref
+    if not os.path.exists(build_ref.GEN_LIB):
+        pytest.skip("reference generators not built here")
+    st, n, T, bx, by, bz, E, steps = "jacobi-3d", 16, 1, 4, 1, 4, 4, 3
+    g = O.ref_geometry(st, n, T, bx, by, bz, E)
+    P, pad, real = g["padded_size"], g["padding"], g["real_size"]
+    x = O.fill_ref(3, P, pad, pad + real, 2024, 1)
+    lib = build_ref.build_kernel_case(st, n, T, bx, by, bz, E, steps)
+    want = O.ref_kernel_run(lib, x, [], T=T, steps=steps,
+                            nb=[g["num_blocks_x"], g["num_blocks_y"], g["num_blocks_z"]],
+                            bs=[bx, by, bz])[0]
+    got = O.sweep_f32(st, x, steps=steps, lo=pad, hi=pad + real, variant=O.VARIANT_REF,
+                      coef=float(np.float32(0.143)))[0]
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))

@@ -2,9 +2,11 @@
 CPU oracle on identical seeded inputs.
 
 Linear stencils (the Jacobi family, both Poisson variants, both FDTD
-variants) must match bit for bit: the library is built with -fmad=false and
-keeps the oracle's operand order.  Stencils with a 1/sqrt term use the GPU
-rsqrt (as the reference kernels do) against 1/sqrt on the CPU; their
+variants) and cs-3d (whose 1/sqrt terms are double expressions in the
+reference's text, IEEE on both sides) must match bit for bit: the library is
+built with -fmad=false and keeps the oracle's operand order.  The other
+stencils with a 1/sqrt term use the GPU's float rsqrt (as the reference
+kernels use OpenCL rsqrt) against a correctly rounded 1/sqrt on the CPU; their
 tolerance is stated per stencil below.
 """
 import numpy as np
@@ -14,12 +16,16 @@ import oracle as O
 import ots
 
 EXACT = {"jacobi-1d", "jacobi-1d-5pt", "jacobi-1d-7pt", "jacobi-2d", "jacobi-3d", "poisson-2d",
-         "poisson-3d", "fdtd-2d"}
-# max |gpu - cpu| / max(|cpu|, 1) after the step counts used here.  rsqrtf
-# is within 2 ulp per call; gradient's 1/sqrt(1e-4 + sum d^2) amplifies that
-# by its sensitivity to the differences d (measured 2.2e-5 on B200).
+         "poisson-3d", "fdtd-2d", "cs-3d"}
+# Bound on max |gpu - cpu| / max(|cpu|, 1) after the step counts used here:
+# a relative error where |cpu| >= 1 and an ABSOLUTE error where |cpu| < 1
+# (the floor of 1 keeps cells near zero from dividing by ~0).  Rician and TV
+# values lie in [0, 1) on these inputs, so theirs is an absolute bound.
+# rsqrtf is within 2 ulp per call; gradient's 1/sqrt(1e-4 + sum d^2)
+# amplifies that by its sensitivity to the differences d (measured 2.2e-5 on
+# B200).
 RTOL = {"gradient-2d": 1e-4, "gradient-3d": 1e-4, "rician-denoise-2d": 2e-5,
-        "cdsc-tv-update-2d": 2e-5, "cs-3d": 2e-5}
+        "cdsc-tv-update-2d": 2e-5}
 
 
 def inputs(plan, seed):
