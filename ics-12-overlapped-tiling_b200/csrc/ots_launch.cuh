@@ -17,6 +17,7 @@
 
 #include "ots_stream.cuh"
 #include "ots_stream2d.cuh"
+#include "ots_stream3p.cuh"
 #include "ots_stream1d.cuh"
 #include "ots_tile.cuh"
 
@@ -41,6 +42,8 @@ using Occ2dFn = cudaError_t (*)(int*);
 // stream kernel queries take the cluster flag (the clustered instantiation)
 using StreamAttrFn = cudaError_t (*)(cudaFuncAttributes*, bool);
 using StreamOccFn = cudaError_t (*)(int*, int, size_t, bool);
+using Occ3pFn = cudaError_t (*)(int*, int, size_t);
+constexpr int kMaxT3p = 4;  // packed 3D stream kernel levels
 
 struct StencilKernels {
   TileLaunch tile[3][kMaxE + 1] = {};  // [E axis][E]
@@ -53,6 +56,10 @@ struct StencilKernels {
   StreamAttrFn stream_attr[kMaxT + 1][3] = {};
   StreamOccFn stream_occ[kMaxT + 1][3] = {};
   bool has_stream = false;
+  // packed-FP32 3D stream kernel (ots_stream3p.cuh): [T <= kMaxT3p][E index]
+  StreamLaunch stream3p[kMaxT3p + 1][3] = {};
+  AttrFn stream3p_attr[kMaxT3p + 1][3] = {};
+  Occ3pFn stream3p_occ[kMaxT3p + 1][3] = {};
   Stream2dLaunch stream2d[kMaxT + 1] = {};  // [T], 2D star stencils
   AttrFn stream2d_attr[kMaxT + 1] = {};
   Occ2dFn stream2d_occ[kMaxT + 1] = {};
@@ -183,6 +190,37 @@ cudaError_t occ_stream(int* blocks, int threads, size_t smem, bool cl) {
             : occ_stream_k<Op, T, E, false>(blocks, threads, smem);
 }
 
+template <class Op, int T, int E>
+cudaError_t launch_stream3p(const CUtensorMap& m, const StreamParams& p, dim3 g, dim3 b,
+                            size_t smem, cudaStream_t s) {
+  static std::atomic<size_t> cached{0};
+  cudaError_t e = ensure_smem(stream3p_kernel<Op, T, E>, smem, cached);
+  if (e != cudaSuccess) return e;
+  return launch_k(stream3p_kernel<Op, T, E>, g, b, smem, s, 1, m, p);
+}
+
+template <class Op, int T, int E>
+cudaError_t attr_stream3p(cudaFuncAttributes* a) {
+  return cudaFuncGetAttributes(a, stream3p_kernel<Op, T, E>);
+}
+
+template <class Op, int T, int E>
+cudaError_t occ_stream3p(int* blocks, int threads, size_t smem) {
+  static std::atomic<size_t> cached{0};
+  cudaError_t e = ensure_smem(stream3p_kernel<Op, T, E>, smem, cached);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, stream3p_kernel<Op, T, E>,
+                                                       threads, smem);
+}
+
+template <class Op, int EI, int... Ts>
+void fill_stream3p_e(StencilKernels& k, std::integer_sequence<int, Ts...>) {
+  ((k.stream3p[Ts + 1][EI] = &launch_stream3p<Op, Ts + 1, kStreamEs[EI]>,
+    k.stream3p_attr[Ts + 1][EI] = &attr_stream3p<Op, Ts + 1, kStreamEs[EI]>,
+    k.stream3p_occ[Ts + 1][EI] = &occ_stream3p<Op, Ts + 1, kStreamEs[EI]>),
+   ...);
+}
+
 template <class Op, int EAX, int... Es>
 void fill_tile(StencilKernels& k, std::integer_sequence<int, Es...>) {
   ((k.tile[EAX][Es + 1] = &launch_tile<Op, Es + 1, EAX>,
@@ -308,6 +346,10 @@ StencilKernels make_kernels_with_stream() {
   fill_stream_e<Op, 1>(k, std::make_integer_sequence<int, kMaxT>{});
   fill_stream_e<Op, 2>(k, std::make_integer_sequence<int, kMaxT>{});
   k.has_stream = true;
+  if constexpr (Op::PACKED && Op::NA == 0) {  // the packed kernel: seven-point Jacobi
+    fill_stream3p_e<Op, 1>(k, std::make_integer_sequence<int, kMaxT3p>{});
+    fill_stream3p_e<Op, 2>(k, std::make_integer_sequence<int, kMaxT3p>{});
+  }
   return k;
 }
 

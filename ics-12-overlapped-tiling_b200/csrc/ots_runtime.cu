@@ -182,6 +182,7 @@ struct Stream2dCfg {
 
 struct StreamCfg {
   int T = 0, E = 0, eidx = 0, bx = 0, by = 0;
+  bool packed = false;     // the packed-FP32 kernel (ots_stream3p.cuh)
   int cy = 1;              // CTAs per cluster along y (their tiles stack into one)
   int tx = 0, ty = 0, rpbx = 0, rpby = 0, zseg = 0;
   int nbx = 0, nby = 0, nbz = 0;
@@ -238,8 +239,10 @@ ots_status derive(const ots_params* p, ots_geometry* g, const StencilInfo** info
   if (!p) return fail(OTS_ERR_INVALID_ARGUMENT, "params is NULL");
   if (p->stencil < 0 || p->stencil >= OTS_NUM_STENCILS)
     return fail(OTS_ERR_INVALID_ARGUMENT, "unknown stencil id %d", p->stencil);
-  for (int i = 0; i < 6; ++i)
+  for (int i = 0; i < 5; ++i)
     if (p->reserved[i] != 0) return fail(OTS_ERR_INVALID_ARGUMENT, "reserved fields must be 0");
+  if (p->stream_impl < 0 || p->stream_impl > 1)
+    return fail(OTS_ERR_INVALID_ARGUMENT, "stream_impl must be 0 or 1 (got %d)", p->stream_impl);
   if (p->cluster_y < 0 || p->cluster_y > 8)
     return fail(OTS_ERR_INVALID_ARGUMENT, "cluster_y must be 0..8 (got %d)", p->cluster_y);
   const StencilInfo& si = kInfo[p->stencil];
@@ -427,7 +430,9 @@ ots_status derive_stream(const ots_plan* pl, int T, StreamCfg* c) {
   c->ty = c->E * c->by;
   c->rpbx = c->tx - 2 * hx;
   c->rpby = c->cy * c->ty - 2 * hy;  // one y halo per cluster tile
-  const int maxthr = T * c->E >= 8 ? 256 : 512;
+  c->packed = p.stream_impl != 1 && c->cy == 1 && T <= ots::kMaxT3p && pl->K &&
+              pl->K->stream3p[T][eidx] != nullptr && c->bx * c->by <= ots::kStream3pThreads;
+  const int maxthr = c->packed ? ots::kStream3pThreads : (T * c->E >= 8 ? 256 : 512);
   if (c->bx != 8 && c->bx != 16 && c->bx != 32)
     return fail(OTS_ERR_UNSUPPORTED, "stream kernel block x must be 8, 16 or 32 (got %d)", c->bx);
   if ((c->bx * c->by) % 32 != 0)
@@ -444,7 +449,8 @@ ots_status derive_stream(const ots_plan* pl, int T, StreamCfg* c) {
     return fail(OTS_ERR_INVALID_GEOMETRY,
                 "Consistency error! stream tile %d x %d leaves no interior at T=%d", c->tx, c->ty,
                 T);
-  c->smem = ots::stream_smem_bytes(T, c->tx, c->ty, c->cy, pl->info->na);
+  c->smem = c->packed ? ots::stream3p_smem_bytes(T, c->tx, c->ty, c->by)
+                      : ots::stream_smem_bytes(T, c->tx, c->ty, c->cy, pl->info->na);
   if (c->smem > pl->smem_optin)
     return fail(OTS_ERR_SMEM_TOO_LARGE,
                 "Not enough local memory for even one block! (%zu > %zu bytes)", c->smem,
@@ -453,7 +459,11 @@ ots_status derive_stream(const ots_plan* pl, int T, StreamCfg* c) {
   c->nbx = ceil_div(n, c->rpbx);
   c->nby = ceil_div(n, c->rpby);
   int per_sm = 1;
-  if (pl->K && pl->K->stream_occ[T][eidx]) {
+  if (c->packed) {
+    int b = 0;
+    if (pl->K->stream3p_occ[T][eidx](&b, c->bx * c->by, c->smem) == cudaSuccess && b > 0)
+      per_sm = b;
+  } else if (pl->K && pl->K->stream_occ[T][eidx]) {
     int b = 0;
     if (pl->K->stream_occ[T][eidx](&b, c->bx * c->by, c->smem, c->cy > 1) == cudaSuccess && b > 0)
       per_sm = b;
@@ -669,12 +679,19 @@ void fill_geometry_for_kernel(ots_plan* pl) {
       g.useful_ratio = (n * n * n) / ((double)c.tx * c.cy * c.ty * c.nbx * c.nby *
                                       (double)c.nbz * (c.zseg + 2 * c.T));
     }
-    if (pl->K->stream_attr[c.T][c.eidx] && pl->K->stream_attr[c.T][c.eidx](&a, c.cy > 1) == cudaSuccess)
-      g.registers = a.numRegs;
     int b = 0;
-    if (pl->K->stream_occ[c.T][c.eidx] &&
-        pl->K->stream_occ[c.T][c.eidx](&b, c.bx * c.by, c.smem, c.cy > 1) == cudaSuccess)
-      g.ctas_per_sm = b;
+    if (c.packed) {
+      if (pl->K->stream3p_attr[c.T][c.eidx](&a) == cudaSuccess) g.registers = a.numRegs;
+      if (pl->K->stream3p_occ[c.T][c.eidx](&b, c.bx * c.by, c.smem) == cudaSuccess)
+        g.ctas_per_sm = b;
+    } else {
+      if (pl->K->stream_attr[c.T][c.eidx] &&
+          pl->K->stream_attr[c.T][c.eidx](&a, c.cy > 1) == cudaSuccess)
+        g.registers = a.numRegs;
+      if (pl->K->stream_occ[c.T][c.eidx] &&
+          pl->K->stream_occ[c.T][c.eidx](&b, c.bx * c.by, c.smem, c.cy > 1) == cudaSuccess)
+        g.ctas_per_sm = b;
+    }
   } else if (g.kernel == OTS_KERNEL_PLAIN) {
     // one cell per thread, blocks of 256 x 1 (1D) or 32 x 8 x 1, one step
     // per launch, no shared memory and no redundant cells
@@ -837,8 +854,12 @@ ots_status enqueue_run(ots_plan* pl, int kernel) {
         if (st == OTS_OK && pl->info->na) st = make_tmap(pl, c, pl->aux[0], &sp.amap);
         if (st != OTS_OK) return st;
       }
-      e = pl->K->stream[Tl][c.eidx](m, sp, dim3(c.nbx * c.nby, c.nbz * c.cy, 1), dim3(c.bx, c.by, 1),
-                                    c.smem, pl->stream);
+      if (c.packed)
+        e = pl->K->stream3p[Tl][c.eidx](m, sp, dim3(c.nbx * c.nby, c.nbz, 1), dim3(c.bx, c.by, 1),
+                                        c.smem, pl->stream);
+      else
+        e = pl->K->stream[Tl][c.eidx](m, sp, dim3(c.nbx * c.nby, c.nbz * c.cy, 1),
+                                      dim3(c.bx, c.by, 1), c.smem, pl->stream);
       pl->cur ^= 1;
     }
   } else if (kernel == OTS_KERNEL_TEX) {

@@ -1,0 +1,340 @@
+// ots_stream3p.cuh -- z-streamed overlapped time tile for the 3D seven-point
+// Jacobi stencil with packed FP32 arithmetic.
+//
+// Same scheme and results as stream_kernel (ots_stream.cuh): a CTA owns an
+// x/y tile (4 x-cells and E rows per thread, halos of round4(T) columns and T
+// rows), walks a z segment plane by plane with all T levels in flight, input
+// planes arrive by TMA into a ring of shared stages, x neighbours travel by
+// shuffle and y neighbours through shared rows, level T writes its plane
+// straight to global memory.  What differs is the arithmetic layout, chosen
+// for the sm_100 packed FP32 instructions (add.rn.f32x2 / mul.rn.f32x2: two
+// IEEE round-to-nearest operations in one instruction, bit for bit the
+// scalar results):
+//
+//   * a thread's row of 4 cells v0..v3 is held as two 64-bit register pairs,
+//     (v0, v2) and (v1, v3).  Every operand of the seven-point sum except two
+//     is then a whole pair: the centre, the rows above and below and the
+//     planes below and above (same x), and the x neighbour inside the thread
+//     ((v1, v3) is the right neighbour of (v0, v2), which is the left
+//     neighbour of (v1, v3)).  Only (v0, v2)'s left neighbour (v-1, v1) and
+//     (v1, v3)'s right neighbour (v2, v4) are assembled, each from one
+//     shuffled and one own value;
+//   * the rows other threads read (a thread's first and last row) go through
+//     a compact exchange buffer in this pair order, so they load straight into
+//     pairs (ld.shared.v2.b64);
+//   * the last level's final multiply is scalar, so its results land in
+//     natural x order for one 16-byte store per row.
+//
+// The rings hold 3 planes per level and 4E cells per plane as pairs: at E=4
+// and T=4 that is 192 registers, so one CTA of 256 threads runs per SM.
+//
+// Every mbarrier wait is bounded (p.wait_ns); on a timeout the CTA records
+// the error word, drains its own copies still in flight (bounded by time
+// only) and all its threads leave together.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "ots_stream.cuh"
+
+namespace ots {
+
+// ---- packed FP32 pairs in 64-bit registers --------------------------------
+__device__ __forceinline__ uint64_t p2_make(float lo, float hi) {
+  uint64_t d;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(lo), "f"(hi));
+  return d;
+}
+__device__ __forceinline__ float p2_lo(uint64_t a) {
+  float lo, hi;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a));
+  return lo;
+}
+__device__ __forceinline__ float p2_hi(uint64_t a) {
+  float lo, hi;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a));
+  return hi;
+}
+__device__ __forceinline__ uint64_t p2_add(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t p2_mul(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+// 16 bytes of shared memory as two pairs, and back
+__device__ __forceinline__ void p2_lds(const float* a, uint64_t& x, uint64_t& y) {
+  const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(a);
+  x = v.x;
+  y = v.y;
+}
+__device__ __forceinline__ void p2_sts(float* a, uint64_t x, uint64_t y) {
+  *reinterpret_cast<ulonglong2*>(a) = make_ulonglong2(x, y);
+}
+// 16 bytes of shared memory in natural order (v0, v1, v2, v3) as the pairs
+// (v0, v2) and (v1, v3)
+__device__ __forceinline__ void p2_lds_nat(const float* a, uint64_t& x, uint64_t& y) {
+  const float4 v = *reinterpret_cast<const float4*>(a);
+  x = p2_make(v.x, v.z);
+  y = p2_make(v.y, v.w);
+}
+
+// Shared layout of the packed kernel (bytes, every piece 128-byte aligned):
+//   NST ring stages of TX x TY floats (the TMA boxes),
+//   exchange rows: levels 1 .. T-1, 2 parities, BY thread rows, 2 rows (the
+//   thread row's first and last), TX floats each,
+//   NST mbarriers.
+constexpr int kStream3pStages = 8;
+constexpr int kStream3pThreads = 256;
+
+__host__ __device__ inline size_t stream3p_stage_bytes(int TX, int TY) {
+  return (size_t)stream_plane_stride(TX, TY) * sizeof(float);
+}
+__host__ __device__ inline size_t stream3p_xbuf_bytes(int T, int TX, int BY) {
+  return (size_t)(T > 1 ? T - 1 : 0) * 2 * BY * 2 * TX * sizeof(float);
+}
+__host__ __device__ inline size_t stream3p_smem_bytes(int T, int TX, int TY, int BY) {
+  return (size_t)kStream3pStages * stream3p_stage_bytes(TX, TY) + stream3p_xbuf_bytes(T, TX, BY) +
+         (size_t)kStream3pStages * 8 + 128;
+}
+
+// blockDim.x (threads along x) must be 8, 16 or 32 so that a warp holds whole
+// thread rows (the x neighbours a shuffle cannot reach are tile-edge halo
+// cells); blockDim.x * blockDim.y <= 256.  Grid: blockIdx.x = x/y tile,
+// blockIdx.y = z segment (p.zseg planes).
+template <class Op, int T, int E>
+__global__ void __launch_bounds__(kStream3pThreads, 1)
+    stream3p_kernel(const __grid_constant__ CUtensorMap tmap,
+                    const __grid_constant__ StreamParams p) {
+  constexpr int V = 4;
+  constexpr int HX = StreamGeom<T>::HX, HY = StreamGeom<T>::HY;
+  constexpr int NST = kStream3pStages, LA = NST - 2;
+  extern __shared__ __align__(128) float smem[];
+  const int BX = blockDim.x, BY = blockDim.y;
+  const int TX = V * BX, TY = E * BY;
+  const int PL = stream_plane_stride(TX, TY);  // floats per stage
+  const int rpbx = TX - 2 * HX, rpby = TY - 2 * HY;
+  const int tid = threadIdx.x + BX * threadIdx.y;
+  const int XS = BY * 2 * TX;                   // floats per exchange buffer
+  float* const xbase = smem + NST * PL;         // exchange buffers
+  uint64_t* const bars =
+      reinterpret_cast<uint64_t*>(xbase + (T > 1 ? (T - 1) * 2 * XS : 0));
+  const unsigned box_bytes = (unsigned)(TX * TY) * sizeof(float);
+  const int n2 = p.L.n2;
+  grid_dependency_sync();
+
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int lx = V * tx, ly = E * ty;
+  // shared offsets (floats) of this thread's pieces: its rows in a stage,
+  // the rows above / below it in a stage (clamped at the tile edge, where
+  // the value is never used), its first / last row and the rows above /
+  // below it in an exchange buffer
+  const int o_row0 = ly * TX + lx;
+  const int o_above = (ly > 0 ? ly - 1 : 0) * TX + lx;
+  const int o_below = (ly + E < TY ? ly + E : TY - 1) * TX + lx;
+  const int xo_top = (ty * 2 + 0) * TX + lx;
+  const int xo_bot = (ty * 2 + 1) * TX + lx;
+  const int xo_above = ((ty > 0 ? ty - 1 : ty) * 2 + 1) * TX + lx;
+  const int xo_below = ((ty + 1 < BY ? ty + 1 : ty) * 2 + 0) * TX + lx;
+
+  if (tid == 0) {
+    for (int s = 0; s < NST; ++s) mbar_init(&bars[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+
+  const int seg = (int)blockIdx.y;
+  const int tile = (int)blockIdx.x;
+  const int zs = seg * p.zseg;
+  const int ze = min(n2, zs + p.zseg);
+  const int tyi = tile / p.ntx, txi = tile - tyi * p.ntx;
+  const int tx0 = txi * rpbx - HX;  // multiple of 4 (TMA x alignment)
+  const int ty0 = tyi * rpby - HY;
+  const int kb = zs - T, nit = (ze - zs) + 2 * T;
+  const int gx = tx0 + lx, gy = ty0 + ly;
+  // cells of this thread inside the domain in x/y: bit (e * 4 + v)
+  unsigned xyin = 0;
+#pragma unroll
+  for (int e = 0; e < E; ++e)
+#pragma unroll
+    for (int v = 0; v < V; ++v)
+      if ((unsigned)(gx + v) < (unsigned)p.L.n0 && (unsigned)(gy + e) < (unsigned)p.L.n1)
+        xyin |= 1u << (e * V + v);
+  const bool xyall = xyin == ((1u << (E * V)) - 1u);
+  // level T stores: this thread's columns in the tile interior; rows whose
+  // tile row lies in the interior
+  const bool st_x = lx >= HX && lx < HX + rpbx && gx < p.L.n0;
+  unsigned st_rows = 0;
+#pragma unroll
+  for (int e = 0; e < E; ++e)
+    if (ly + e >= HY && ly + e < HY + rpby && gy + e < p.L.n1) st_rows |= 1u << e;
+  const bool st_any = st_x && st_rows != 0;
+  const bool st_full4 = gx + 3 < p.L.n0;  // all four columns inside (one 16-byte store)
+  float* const gbase = p.out + (int64_t)gy * p.L.sy + gx;  // used only where gx, gy >= 0
+  const int64_t gsz = p.L.sz, gsy = p.L.sy;
+  const uint64_t coef2 = p2_make(p.op.coef, p.op.coef);
+  const float coef = p.op.coef;
+
+  // test hook: CTA 0 arms the stage of running plane hold_plane but never
+  // loads it, so that plane's wait can only run out (a flag nothing sets)
+  const bool hold_cta = p.hold_plane >= 0 && blockIdx.x == 0 && blockIdx.y == 0;
+  if (tid == 0) {
+    for (int j = 0; j < LA && j < nit; ++j) {
+      mbar_arrive_expect_tx(&bars[j], box_bytes);
+      if (!(hold_cta && j == p.hold_plane))
+        tma_load_3d(smem + j * PL, &tmap, tx0, ty0, kb + j, &bars[j]);
+    }
+  }
+
+  // R[t][slot][e][pair]: level t's (0 = input) three newest planes
+  uint64_t R[T][3][E][2];
+#pragma unroll
+  for (int t = 0; t < T; ++t)
+#pragma unroll
+    for (int s = 0; s < 3; ++s)
+#pragma unroll
+      for (int e = 0; e < E; ++e) R[t][s][e][0] = R[t][s][e][1] = 0ull;
+
+  bool ok = true;
+  int fail_r = -1;
+
+  auto step = [&](auto ph, int r) -> bool {
+    constexpr int PH = decltype(ph)::value;
+    constexpr int SN = PH, SC = (PH + 2) % 3, SM = (PH + 1) % 3;  // newest, centre, z-1
+    const int k = kb + r;
+    const int st = r & (NST - 1);
+    const bool to = !mbar_wait_bounded(&bars[st], (r / NST) & 1, p.err, p.wait_ns);
+    if (__syncthreads_or(to)) {
+      fail_r = r;
+      return false;
+    }
+    if (tid == 0 && r + LA < nit) {
+      const int s2 = (r + LA) & (NST - 1);
+      mbar_arrive_expect_tx(&bars[s2], box_bytes);
+      if (!(hold_cta && r + LA == p.hold_plane))
+        tma_load_3d(smem + s2 * PL, &tmap, tx0, ty0, k + LA, &bars[s2]);
+    }
+    // level 0: the input plane k into registers (pair order)
+    const float* const sk = smem + st * PL;
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+      p2_lds_nat(sk + o_row0 + e * TX, R[0][SN][e][0], R[0][SN][e][1]);
+    const float* const pk = smem + ((r + NST - 1) & (NST - 1)) * PL;  // plane k-1
+    float* const xr = xbase + ((r - 1) & 1) * XS;  // exchange rows written at r-1
+    float* const xw = xbase + (r & 1) * XS;        // exchange rows written now
+#pragma unroll
+    for (int t = 1; t <= T; ++t) {
+      const int q = k - t;
+      uint64_t (&L)[3][E][2] = R[t - 1];
+      // rows above / below of level t-1's plane q (other threads' rows)
+      uint64_t ab0, ab1, be0, be1;
+      if (t == 1) {
+        p2_lds_nat(pk + o_above, ab0, ab1);
+        p2_lds_nat(pk + o_below, be0, be1);
+      } else {
+        const float* const xl = xr + (t - 2) * 2 * XS;
+        p2_lds(xl + xo_above, ab0, ab1);
+        p2_lds(xl + xo_below, be0, be1);
+      }
+      const bool zin = (unsigned)q < (unsigned)n2;
+      uint64_t O[E][2];
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const uint64_t c0 = L[SC][e][0], c1 = L[SC][e][1];  // (v0, v2), (v1, v3)
+        // x neighbours: (v-1, v1) and (v2, v4); v-1 / v4 from the lanes beside
+        const float left = __shfl_up_sync(0xffffffffu, p2_hi(c1), 1);
+        const float right = __shfl_down_sync(0xffffffffu, p2_lo(c0), 1);
+        const uint64_t xm0 = p2_make(left, p2_lo(c1));
+        const uint64_t xp1 = p2_make(p2_hi(c0), right);
+        const uint64_t ym0 = e > 0 ? L[SC][e > 0 ? e - 1 : 0][0] : ab0;
+        const uint64_t ym1 = e > 0 ? L[SC][e > 0 ? e - 1 : 0][1] : ab1;
+        const uint64_t yp0 = e < E - 1 ? L[SC][e < E - 1 ? e + 1 : 0][0] : be0;
+        const uint64_t yp1 = e < E - 1 ? L[SC][e < E - 1 ? e + 1 : 0][1] : be1;
+        // x-1, c, x+1, y-1, y+1, z-1, z+1 (opencl/jacobi-3d/jacobi-3d.cpp:282-304)
+        uint64_t s0 = p2_add(xm0, c0);
+        uint64_t s1 = p2_add(c0, c1);
+        s0 = p2_add(s0, c1);
+        s1 = p2_add(s1, xp1);
+        s0 = p2_add(s0, ym0);
+        s1 = p2_add(s1, ym1);
+        s0 = p2_add(s0, yp0);
+        s1 = p2_add(s1, yp1);
+        s0 = p2_add(s0, L[SM][e][0]);
+        s1 = p2_add(s1, L[SM][e][1]);
+        s0 = p2_add(s0, L[SN][e][0]);
+        s1 = p2_add(s1, L[SN][e][1]);
+        O[e][0] = s0;
+        O[e][1] = s1;
+      }
+      if (t < T) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          O[e][0] = p2_mul(coef2, O[e][0]);
+          O[e][1] = p2_mul(coef2, O[e][1]);
+        }
+        if (!(zin && xyall)) {  // domain edge: zero the cells outside
+#pragma unroll
+          for (int e = 0; e < E; ++e) {
+            const unsigned m = zin ? (xyin >> (e * V)) & 0xFu : 0u;
+            O[e][0] = p2_make((m & 1u) ? p2_lo(O[e][0]) : 0.0f, (m & 4u) ? p2_hi(O[e][0]) : 0.0f);
+            O[e][1] = p2_make((m & 2u) ? p2_lo(O[e][1]) : 0.0f, (m & 8u) ? p2_hi(O[e][1]) : 0.0f);
+          }
+        }
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          R[t][SN][e][0] = O[e][0];
+          R[t][SN][e][1] = O[e][1];
+        }
+        // other threads read only this thread's first and last rows
+        float* const xl = xw + (t - 1) * 2 * XS;
+        p2_sts(xl + xo_top, O[0][0], O[0][1]);
+        p2_sts(xl + xo_bot, O[E - 1][0], O[E - 1][1]);
+      } else if (st_any && q >= zs && q < ze) {
+        // level T: final multiply in scalar, natural x order, one store per row
+        float* const dst = gbase + (int64_t)q * gsz;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          if (!((st_rows >> e) & 1u)) continue;
+          const float4 o = make_float4(coef * p2_lo(O[e][0]), coef * p2_lo(O[e][1]),
+                                       coef * p2_hi(O[e][0]), coef * p2_hi(O[e][1]));
+          if (st_full4) {
+            *reinterpret_cast<float4*>(dst + (int64_t)e * gsy) = o;
+          } else {
+            const float ov[4] = {o.x, o.y, o.z, o.w};
+#pragma unroll
+            for (int v = 0; v < V; ++v)
+              if (gx + v < p.L.n0) dst[(int64_t)e * gsy + v] = ov[v];
+          }
+        }
+      }
+    }
+    return true;
+  };
+
+  int r = 0;
+  for (; r + 2 < nit && ok; r += 3) {
+    ok = step(Phase<0>{}, r);
+    if (ok) ok = step(Phase<1>{}, r + 1);
+    if (ok) ok = step(Phase<2>{}, r + 2);
+  }
+  if (ok && r < nit) ok = step(Phase<0>{}, r++);
+  if (ok && r < nit) ok = step(Phase<1>{}, r++);
+  if (!ok) {
+    if (tid == 0) {
+      atomicOr(p.err, 1);
+      // drain this CTA's copies still in flight before leaving, each wait
+      // bounded by time only: planes fail_r .. fail_r + LA - 1 were issued
+      for (int j = fail_r; j < nit && j < fail_r + LA; ++j)
+        mbar_wait_drain(&bars[j & (NST - 1)], (j / NST) & 1, p.wait_ns);
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace ots

@@ -56,7 +56,8 @@ class Params(ctypes.Structure):
                 ("engine", ctypes.c_int32), ("kernel", ctypes.c_int32),
                 ("variant", ctypes.c_int32), ("phase_limit", ctypes.c_int32),
                 ("coef", ctypes.c_float), ("h2", ctypes.c_float), ("device", ctypes.c_int32),
-                ("cluster_y", ctypes.c_int32), ("reserved", ctypes.c_int32 * 6)]
+                ("cluster_y", ctypes.c_int32), ("stream_impl", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 5)]
 
 
 class Geometry(ctypes.Structure):
@@ -180,7 +181,7 @@ def _fptrs(arrays):
 
 def make_params(stencil, n, steps, T=1, bx=16, by=16, bz=1, E=1, engine=ENGINE_NATIVE,
                 kernel=KERNEL_AUTO, variant=VARIANT_BASELINE, phase_limit=0, coef=0.0, h2=0.0,
-                device=0, cy=1):
+                device=0, cy=1, impl=0):
     p = Params()
     p.stencil = SID[stencil] if isinstance(stencil, str) else int(stencil)
     p.problem_size, p.time_steps, p.time_tile = n, steps, T
@@ -189,6 +190,7 @@ def make_params(stencil, n, steps, T=1, bx=16, by=16, bz=1, E=1, engine=ENGINE_N
     p.kernel = KERNELS[kernel] if isinstance(kernel, str) else kernel
     p.variant, p.phase_limit, p.coef, p.h2, p.device = variant, phase_limit, coef, h2, device
     p.cluster_y = cy
+    p.stream_impl = impl
     return p
 
 

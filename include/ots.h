@@ -123,7 +123,12 @@ typedef struct ots_params {
                                   cluster shares one tile of cluster_y * block_y
                                   * E rows, so the 2T-row y halo is recomputed
                                   once per cluster instead of once per CTA. */
-  int32_t reserved[6];         /* must be zero */
+  int32_t stream_impl;         /* 3D stream kernel implementation: 0 = the
+                                  packed-FP32 kernel where it applies (jacobi-3d,
+                                  E 2 or 4, T <= 4, no clusters, at most 256
+                                  threads), else the scalar one; 1 = always the
+                                  scalar kernel.  Both give identical bits. */
+  int32_t reserved[5];         /* must be zero */
 } ots_params;
 
 /* Derived values: the reference's GeneratorParams fields plus what the

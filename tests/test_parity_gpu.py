@@ -456,3 +456,39 @@ def test_full_size_jacobi_3d_tiled_equals_plain_and_fp64_error():
                         coef=g.coef)[0]
     mr, rms = O.error_vs_f64(got, ref64, g.padding, g.padding + m, floor=1e-6)
     assert mr <= 1e-5, mr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("T", [1, 2, 3, 4])
+@pytest.mark.parametrize("E,bx,by", [(4, 16, 16), (4, 8, 32), (4, 32, 8), (2, 16, 16),
+                                     (2, 32, 8), (4, 16, 6)])
+def test_packed_stream_kernel_matches_oracle(T, E, bx, by):
+    """The packed-FP32 z-streamed kernel (pairs (v0, v2), (v1, v3) in 64-bit
+    registers): bit for bit against the oracle, with n not a multiple of the
+    tile interior, several z segments and a shallower last launch."""
+    g = run_and_check("jacobi-3d", 61, 2 * T + 1, T=T, bx=bx, by=by, bz=1, E=E, kernel="stream")
+    assert g.kernel == ots.KERNEL_STREAM
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,steps,T,E,bx,by", [(130, 9, 4, 4, 16, 16), (97, 7, 3, 4, 16, 16),
+                                               (64, 8, 4, 2, 16, 16), (33, 5, 2, 4, 8, 8),
+                                               (200, 4, 4, 4, 16, 16), (5, 6, 4, 4, 16, 16)])
+def test_packed_and_scalar_stream_kernels_agree_bitwise(n, steps, T, E, bx, by):
+    """stream_impl 0 (packed) and 1 (scalar) on the same plan shape: identical
+    bits, and both equal to the oracle (the reference weight 0.143 too)."""
+    outs = []
+    for impl in (0, 1):
+        with ots.Plan("jacobi-3d", n, steps, T=T, bx=bx, by=by, bz=1, E=E, kernel="stream",
+                      impl=impl) as plan:
+            state, _ = plan.fill_reference(seed=21)
+            plan.upload(state)
+            plan.run()
+            outs.append(plan.download()[0])
+            g = plan.geometry
+    want = O.sweep_f32("jacobi-3d", state, steps=steps, lo=g.padding, hi=g.padding + g.real_size,
+                       coef=g.coef)[0]
+    assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
+    assert np.array_equal(outs[0].view(np.uint32), want.view(np.uint32))
+    run_and_check("jacobi-3d", 45, 6, T=3, bx=16, by=16, bz=1, E=4, kernel="stream",
+                  variant=ots.VARIANT_REF)
