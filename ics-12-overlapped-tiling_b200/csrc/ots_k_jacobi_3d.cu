@@ -4,7 +4,12 @@
 
 namespace ots {
 const StencilKernels& kernels_jacobi_3d() {
-  static const StencilKernels k = make_kernels_with_stream<OpJacobi3D>();
+  static const StencilKernels k = [] {
+    StencilKernels t = make_kernels_with_stream<OpJacobi3D>();
+    fill_stream3p_jacobi_3d_a(t);  // the packed-FP32 stream kernel
+    fill_stream3p_jacobi_3d_b(t);
+    return t;
+  }();
   return k;
 }
 }  // namespace ots

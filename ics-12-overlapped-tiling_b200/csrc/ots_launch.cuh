@@ -56,10 +56,11 @@ struct StencilKernels {
   StreamAttrFn stream_attr[kMaxT + 1][3] = {};
   StreamOccFn stream_occ[kMaxT + 1][3] = {};
   bool has_stream = false;
-  // packed-FP32 3D stream kernel (ots_stream3p.cuh): [T <= kMaxT3p][E index]
-  StreamLaunch stream3p[kMaxT3p + 1][3] = {};
-  AttrFn stream3p_attr[kMaxT3p + 1][3] = {};
-  Occ3pFn stream3p_occ[kMaxT3p + 1][3] = {};
+  // packed-FP32 3D stream kernel (ots_stream3p.cuh): [T <= kMaxT3p][shape
+  // index in kShape3p]
+  StreamLaunch stream3p[kMaxT3p + 1][kShapes3p] = {};
+  AttrFn stream3p_attr[kMaxT3p + 1][kShapes3p] = {};
+  Occ3pFn stream3p_occ[kMaxT3p + 1][kShapes3p] = {};
   Stream2dLaunch stream2d[kMaxT + 1] = {};  // [T], 2D star stencils
   AttrFn stream2d_attr[kMaxT + 1] = {};
   Occ2dFn stream2d_occ[kMaxT + 1] = {};
@@ -190,36 +191,45 @@ cudaError_t occ_stream(int* blocks, int threads, size_t smem, bool cl) {
             : occ_stream_k<Op, T, E, false>(blocks, threads, smem);
 }
 
-template <class Op, int T, int E>
+template <class Op, int T, int SI>
 cudaError_t launch_stream3p(const CUtensorMap& m, const StreamParams& p, dim3 g, dim3 b,
                             size_t smem, cudaStream_t s) {
+  constexpr Shape3p S = kShape3p[SI];
   static std::atomic<size_t> cached{0};
-  cudaError_t e = ensure_smem(stream3p_kernel<Op, T, E>, smem, cached);
+  cudaError_t e = ensure_smem(stream3p_kernel<Op, T, S.E, S.BX, S.BY>, smem, cached);
   if (e != cudaSuccess) return e;
-  return launch_k(stream3p_kernel<Op, T, E>, g, b, smem, s, 1, m, p);
+  return launch_k(stream3p_kernel<Op, T, S.E, S.BX, S.BY>, g, b, smem, s, 1, m, p);
 }
 
-template <class Op, int T, int E>
+template <class Op, int T, int SI>
 cudaError_t attr_stream3p(cudaFuncAttributes* a) {
-  return cudaFuncGetAttributes(a, stream3p_kernel<Op, T, E>);
+  constexpr Shape3p S = kShape3p[SI];
+  return cudaFuncGetAttributes(a, stream3p_kernel<Op, T, S.E, S.BX, S.BY>);
 }
 
-template <class Op, int T, int E>
+template <class Op, int T, int SI>
 cudaError_t occ_stream3p(int* blocks, int threads, size_t smem) {
+  constexpr Shape3p S = kShape3p[SI];
   static std::atomic<size_t> cached{0};
-  cudaError_t e = ensure_smem(stream3p_kernel<Op, T, E>, smem, cached);
+  cudaError_t e = ensure_smem(stream3p_kernel<Op, T, S.E, S.BX, S.BY>, smem, cached);
   if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, stream3p_kernel<Op, T, E>,
-                                                       threads, smem);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      blocks, stream3p_kernel<Op, T, S.E, S.BX, S.BY>, threads, smem);
 }
 
-template <class Op, int EI, int... Ts>
-void fill_stream3p_e(StencilKernels& k, std::integer_sequence<int, Ts...>) {
-  ((k.stream3p[Ts + 1][EI] = &launch_stream3p<Op, Ts + 1, kStreamEs[EI]>,
-    k.stream3p_attr[Ts + 1][EI] = &attr_stream3p<Op, Ts + 1, kStreamEs[EI]>,
-    k.stream3p_occ[Ts + 1][EI] = &occ_stream3p<Op, Ts + 1, kStreamEs[EI]>),
+// One shape of the packed kernel for every T (compiled where it is called,
+// one translation unit per shape group).
+template <class Op, int SI, int... Ts>
+void fill_stream3p_shape(StencilKernels& k, std::integer_sequence<int, Ts...>) {
+  ((k.stream3p[Ts + 1][SI] = &launch_stream3p<Op, Ts + 1, SI>,
+    k.stream3p_attr[Ts + 1][SI] = &attr_stream3p<Op, Ts + 1, SI>,
+    k.stream3p_occ[Ts + 1][SI] = &occ_stream3p<Op, Ts + 1, SI>),
    ...);
 }
+
+// Defined in ots_k_jacobi_3d_p<N>.cu: the packed kernel's table entries.
+void fill_stream3p_jacobi_3d_a(StencilKernels& k);
+void fill_stream3p_jacobi_3d_b(StencilKernels& k);
 
 template <class Op, int EAX, int... Es>
 void fill_tile(StencilKernels& k, std::integer_sequence<int, Es...>) {
@@ -346,10 +356,6 @@ StencilKernels make_kernels_with_stream() {
   fill_stream_e<Op, 1>(k, std::make_integer_sequence<int, kMaxT>{});
   fill_stream_e<Op, 2>(k, std::make_integer_sequence<int, kMaxT>{});
   k.has_stream = true;
-  if constexpr (Op::PACKED && Op::NA == 0) {  // the packed kernel: seven-point Jacobi
-    fill_stream3p_e<Op, 1>(k, std::make_integer_sequence<int, kMaxT3p>{});
-    fill_stream3p_e<Op, 2>(k, std::make_integer_sequence<int, kMaxT3p>{});
-  }
   return k;
 }
 

@@ -183,6 +183,7 @@ struct Stream2dCfg {
 struct StreamCfg {
   int T = 0, E = 0, eidx = 0, bx = 0, by = 0;
   bool packed = false;     // the packed-FP32 kernel (ots_stream3p.cuh)
+  int shape3p = -1;        // its block shape (index in kShape3p)
   int cy = 1;              // CTAs per cluster along y (their tiles stack into one)
   int tx = 0, ty = 0, rpbx = 0, rpby = 0, zseg = 0;
   int nbx = 0, nby = 0, nbz = 0;
@@ -430,9 +431,10 @@ ots_status derive_stream(const ots_plan* pl, int T, StreamCfg* c) {
   c->ty = c->E * c->by;
   c->rpbx = c->tx - 2 * hx;
   c->rpby = c->cy * c->ty - 2 * hy;  // one y halo per cluster tile
+  c->shape3p = ots::shape3p_index(c->E, c->bx, c->by);
   c->packed = p.stream_impl != 1 && c->cy == 1 && T <= ots::kMaxT3p && pl->K &&
-              pl->K->stream3p[T][eidx] != nullptr && c->bx * c->by <= ots::kStream3pThreads;
-  const int maxthr = c->packed ? ots::kStream3pThreads : (T * c->E >= 8 ? 256 : 512);
+              c->shape3p >= 0 && pl->K->stream3p[T][c->shape3p] != nullptr;
+  const int maxthr = c->packed ? 512 : (T * c->E >= 8 ? 256 : 512);
   if (c->bx != 8 && c->bx != 16 && c->bx != 32)
     return fail(OTS_ERR_UNSUPPORTED, "stream kernel block x must be 8, 16 or 32 (got %d)", c->bx);
   if ((c->bx * c->by) % 32 != 0)
@@ -449,7 +451,7 @@ ots_status derive_stream(const ots_plan* pl, int T, StreamCfg* c) {
     return fail(OTS_ERR_INVALID_GEOMETRY,
                 "Consistency error! stream tile %d x %d leaves no interior at T=%d", c->tx, c->ty,
                 T);
-  c->smem = c->packed ? ots::stream3p_smem_bytes(T, c->tx, c->ty, c->by)
+  c->smem = c->packed ? ots::stream3p_smem_bytes(T, c->tx, c->ty, c->by) + 128
                       : ots::stream_smem_bytes(T, c->tx, c->ty, c->cy, pl->info->na);
   if (c->smem > pl->smem_optin)
     return fail(OTS_ERR_SMEM_TOO_LARGE,
@@ -461,7 +463,7 @@ ots_status derive_stream(const ots_plan* pl, int T, StreamCfg* c) {
   int per_sm = 1;
   if (c->packed) {
     int b = 0;
-    if (pl->K->stream3p_occ[T][eidx](&b, c->bx * c->by, c->smem) == cudaSuccess && b > 0)
+    if (pl->K->stream3p_occ[T][c->shape3p](&b, c->bx * c->by, c->smem) == cudaSuccess && b > 0)
       per_sm = b;
   } else if (pl->K && pl->K->stream_occ[T][eidx]) {
     int b = 0;
@@ -681,8 +683,8 @@ void fill_geometry_for_kernel(ots_plan* pl) {
     }
     int b = 0;
     if (c.packed) {
-      if (pl->K->stream3p_attr[c.T][c.eidx](&a) == cudaSuccess) g.registers = a.numRegs;
-      if (pl->K->stream3p_occ[c.T][c.eidx](&b, c.bx * c.by, c.smem) == cudaSuccess)
+      if (pl->K->stream3p_attr[c.T][c.shape3p](&a) == cudaSuccess) g.registers = a.numRegs;
+      if (pl->K->stream3p_occ[c.T][c.shape3p](&b, c.bx * c.by, c.smem) == cudaSuccess)
         g.ctas_per_sm = b;
     } else {
       if (pl->K->stream_attr[c.T][c.eidx] &&
@@ -855,8 +857,8 @@ ots_status enqueue_run(ots_plan* pl, int kernel) {
         if (st != OTS_OK) return st;
       }
       if (c.packed)
-        e = pl->K->stream3p[Tl][c.eidx](m, sp, dim3(c.nbx * c.nby, c.nbz, 1), dim3(c.bx, c.by, 1),
-                                        c.smem, pl->stream);
+        e = pl->K->stream3p[Tl][c.shape3p](m, sp, dim3(c.nbx * c.nby, c.nbz, 1),
+                                           dim3(c.bx, c.by, 1), c.smem, pl->stream);
       else
         e = pl->K->stream[Tl][c.eidx](m, sp, dim3(c.nbx * c.nby, c.nbz * c.cy, 1),
                                       dim3(c.bx, c.by, 1), c.smem, pl->stream);
@@ -1561,6 +1563,8 @@ ots_status ots_describe(const ots_plan* plan, ots_kv_fn kv, void* user) {
   emit_i("Register Usage", g.registers);
   static const char* kKernel[] = {"auto", "tile", "stream", "plain", "tex"};
   kv("Kernel", kKernel[(g.kernel >= 0 && g.kernel <= 4) ? g.kernel : 0], user);
+  if (g.kernel == OTS_KERNEL_STREAM && g.dims == 3)
+    kv("Stream Arithmetic", plan->scfg.packed ? "packed-fp32" : "scalar", user);
   emit_i("Dynamic Shared Bytes", g.shared_bytes);
   kv("Engine", p.engine == OTS_ENGINE_COMPAT ? "compat" : "native", user);
   kv("Variant", p.variant == OTS_VARIANT_REF ? "ref" : "baseline", user);

@@ -26,7 +26,9 @@
 //     natural x order for one 16-byte store per row.
 //
 // The rings hold 3 planes per level and 4E cells per plane as pairs: at E=4
-// and T=4 that is 192 registers, so one CTA of 256 threads runs per SM.
+// and T=4 that is 192 registers (one CTA of 256 threads per SM), at E=2 96
+// (512 threads).  The block shape is a template argument, so every shared
+// and exchange offset is an immediate.
 //
 // Every mbarrier wait is bounded (p.wait_ns); on a timeout the CTA records
 // the error word, drains its own copies still in flight (bounded by time
@@ -50,11 +52,13 @@ __device__ __forceinline__ uint64_t p2_make(float lo, float hi) {
 __device__ __forceinline__ float p2_lo(uint64_t a) {
   float lo, hi;
   asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a));
+  (void)hi;
   return lo;
 }
 __device__ __forceinline__ float p2_hi(uint64_t a) {
   float lo, hi;
   asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a));
+  (void)lo;
   return hi;
 }
 __device__ __forceinline__ uint64_t p2_add(uint64_t a, uint64_t b) {
@@ -84,47 +88,64 @@ __device__ __forceinline__ void p2_lds_nat(const float* a, uint64_t& x, uint64_t
   y = p2_make(v.y, v.w);
 }
 
-// Shared layout of the packed kernel (bytes, every piece 128-byte aligned):
+// Block shapes instantiated for the packed kernel: {E, BX, BY}.
+struct Shape3p {
+  int E, BX, BY;
+};
+constexpr int kShapes3p = 6;
+constexpr Shape3p kShape3p[kShapes3p] = {{4, 16, 16}, {4, 16, 8}, {4, 8, 16},
+                                         {2, 16, 32}, {2, 32, 16}, {2, 16, 16}};
+inline int shape3p_index(int E, int BX, int BY) {
+  for (int i = 0; i < kShapes3p; ++i)
+    if (kShape3p[i].E == E && kShape3p[i].BX == BX && kShape3p[i].BY == BY) return i;
+  return -1;
+}
+
+// Shared layout (floats unless noted; every piece 128-byte aligned):
 //   NST ring stages of TX x TY floats (the TMA boxes),
 //   exchange rows: levels 1 .. T-1, 2 parities, BY thread rows, 2 rows (the
-//   thread row's first and last), TX floats each,
+//   thread row's first and last, pair order), TX floats each,
 //   NST mbarriers.
-constexpr int kStream3pStages = 8;
-constexpr int kStream3pThreads = 256;
+// NST is 8 where that fits the 227 KB a CTA may use, else 4.
+constexpr size_t kSmemPerCta = 227 * 1024;
+__host__ __device__ constexpr size_t stream3p_stage_floats(int TX, int TY) {
+  return (size_t)(TX * TY + 31) / 32 * 32;
+}
+__host__ __device__ constexpr size_t stream3p_xbuf_floats(int T, int TX, int BY) {
+  return (size_t)(T > 1 ? T - 1 : 0) * 2 * BY * 2 * TX;
+}
+__host__ __device__ constexpr size_t stream3p_bytes(int nst, int T, int TX, int TY, int BY) {
+  return ((size_t)nst * stream3p_stage_floats(TX, TY) + stream3p_xbuf_floats(T, TX, BY)) * 4 +
+         (size_t)nst * 8;
+}
+__host__ __device__ constexpr int stream3p_stages(int T, int TX, int TY, int BY) {
+  return stream3p_bytes(8, T, TX, TY, BY) <= kSmemPerCta ? 8 : 4;
+}
+__host__ __device__ constexpr size_t stream3p_smem_bytes(int T, int TX, int TY, int BY) {
+  return stream3p_bytes(stream3p_stages(T, TX, TY, BY), T, TX, TY, BY);
+}
 
-__host__ __device__ inline size_t stream3p_stage_bytes(int TX, int TY) {
-  return (size_t)stream_plane_stride(TX, TY) * sizeof(float);
-}
-__host__ __device__ inline size_t stream3p_xbuf_bytes(int T, int TX, int BY) {
-  return (size_t)(T > 1 ? T - 1 : 0) * 2 * BY * 2 * TX * sizeof(float);
-}
-__host__ __device__ inline size_t stream3p_smem_bytes(int T, int TX, int TY, int BY) {
-  return (size_t)kStream3pStages * stream3p_stage_bytes(TX, TY) + stream3p_xbuf_bytes(T, TX, BY) +
-         (size_t)kStream3pStages * 8 + 128;
-}
-
-// blockDim.x (threads along x) must be 8, 16 or 32 so that a warp holds whole
-// thread rows (the x neighbours a shuffle cannot reach are tile-edge halo
-// cells); blockDim.x * blockDim.y <= 256.  Grid: blockIdx.x = x/y tile,
-// blockIdx.y = z segment (p.zseg planes).
-template <class Op, int T, int E>
-__global__ void __launch_bounds__(kStream3pThreads, 1)
+// Warps hold whole thread rows (BX = 8, 16 or 32), so the x neighbours a
+// shuffle cannot reach are tile-edge halo cells.  Grid: blockIdx.x = x/y
+// tile, blockIdx.y = z segment (p.zseg planes).
+template <class Op, int T, int E, int BX, int BY>
+__global__ void __launch_bounds__(BX * BY, 1)
     stream3p_kernel(const __grid_constant__ CUtensorMap tmap,
                     const __grid_constant__ StreamParams p) {
   constexpr int V = 4;
   constexpr int HX = StreamGeom<T>::HX, HY = StreamGeom<T>::HY;
-  constexpr int NST = kStream3pStages, LA = NST - 2;
+  constexpr int TX = V * BX, TY = E * BY;
+  constexpr int NST = stream3p_stages(T, TX, TY, BY), LA = NST - 2;
+  constexpr int PL = (int)stream3p_stage_floats(TX, TY);  // floats per stage
+  constexpr int XS = BY * 2 * TX;                          // floats per exchange buffer
+  constexpr int rpbx = TX - 2 * HX, rpby = TY - 2 * HY;
+  constexpr unsigned box_bytes = (unsigned)(TX * TY) * sizeof(float);
+  static_assert(BX == 8 || BX == 16 || BX == 32, "a warp holds whole thread rows");
+  static_assert(rpbx >= 4 && rpby >= 1, "the tile keeps an interior");
   extern __shared__ __align__(128) float smem[];
-  const int BX = blockDim.x, BY = blockDim.y;
-  const int TX = V * BX, TY = E * BY;
-  const int PL = stream_plane_stride(TX, TY);  // floats per stage
-  const int rpbx = TX - 2 * HX, rpby = TY - 2 * HY;
+  float* const xbase = smem + NST * PL;  // exchange buffers
+  uint64_t* const bars = reinterpret_cast<uint64_t*>(xbase + (T > 1 ? (T - 1) * 2 * XS : 0));
   const int tid = threadIdx.x + BX * threadIdx.y;
-  const int XS = BY * 2 * TX;                   // floats per exchange buffer
-  float* const xbase = smem + NST * PL;         // exchange buffers
-  uint64_t* const bars =
-      reinterpret_cast<uint64_t*>(xbase + (T > 1 ? (T - 1) * 2 * XS : 0));
-  const unsigned box_bytes = (unsigned)(TX * TY) * sizeof(float);
   const int n2 = p.L.n2;
   grid_dependency_sync();
 
@@ -176,10 +197,14 @@ __global__ void __launch_bounds__(kStream3pThreads, 1)
     if (ly + e >= HY && ly + e < HY + rpby && gy + e < p.L.n1) st_rows |= 1u << e;
   const bool st_any = st_x && st_rows != 0;
   const bool st_full4 = gx + 3 < p.L.n0;  // all four columns inside (one 16-byte store)
-  float* const gbase = p.out + (int64_t)gy * p.L.sy + gx;  // used only where gx, gy >= 0
   const int64_t gsz = p.L.sz, gsy = p.L.sy;
+  // level T of iteration r writes plane kb + r - T; the pointer walks one
+  // plane per iteration and is dereferenced only for planes in [zs, ze)
+  // (where gx, gy and the plane index are all inside the array)
+  float* gptr = p.out + (int64_t)gy * gsy + gx + (int64_t)(kb - T) * gsz;
   const uint64_t coef2 = p2_make(p.op.coef, p.op.coef);
   const float coef = p.op.coef;
+  const int zlo = zs + T, zhi = ze + T;  // iterations' k range whose level-T plane is stored
 
   // test hook: CTA 0 arms the stage of running plane hold_plane but never
   // loads it, so that plane's wait can only run out (a flag nothing sets)
@@ -221,13 +246,14 @@ __global__ void __launch_bounds__(kStream3pThreads, 1)
         tma_load_3d(smem + s2 * PL, &tmap, tx0, ty0, k + LA, &bars[s2]);
     }
     // level 0: the input plane k into registers (pair order)
-    const float* const sk = smem + st * PL;
+    const float* const sk = smem + st * PL + o_row0;
 #pragma unroll
-    for (int e = 0; e < E; ++e)
-      p2_lds_nat(sk + o_row0 + e * TX, R[0][SN][e][0], R[0][SN][e][1]);
+    for (int e = 0; e < E; ++e) p2_lds_nat(sk + e * TX, R[0][SN][e][0], R[0][SN][e][1]);
     const float* const pk = smem + ((r + NST - 1) & (NST - 1)) * PL;  // plane k-1
-    float* const xr = xbase + ((r - 1) & 1) * XS;  // exchange rows written at r-1
-    float* const xw = xbase + (r & 1) * XS;        // exchange rows written now
+    const int par = r & 1;
+    const float* const xr = xbase + (par ^ 1) * XS;  // exchange rows written at r-1
+    float* const xw = xbase + par * XS;               // exchange rows written now
+    const bool store = st_any && k >= zlo && k < zhi;
 #pragma unroll
     for (int t = 1; t <= T; ++t) {
       const int q = k - t;
@@ -242,7 +268,6 @@ __global__ void __launch_bounds__(kStream3pThreads, 1)
         p2_lds(xl + xo_above, ab0, ab1);
         p2_lds(xl + xo_below, be0, be1);
       }
-      const bool zin = (unsigned)q < (unsigned)n2;
       uint64_t O[E][2];
 #pragma unroll
       for (int e = 0; e < E; ++e) {
@@ -278,6 +303,7 @@ __global__ void __launch_bounds__(kStream3pThreads, 1)
           O[e][0] = p2_mul(coef2, O[e][0]);
           O[e][1] = p2_mul(coef2, O[e][1]);
         }
+        const bool zin = (unsigned)q < (unsigned)n2;
         if (!(zin && xyall)) {  // domain edge: zero the cells outside
 #pragma unroll
           for (int e = 0; e < E; ++e) {
@@ -295,25 +321,25 @@ __global__ void __launch_bounds__(kStream3pThreads, 1)
         float* const xl = xw + (t - 1) * 2 * XS;
         p2_sts(xl + xo_top, O[0][0], O[0][1]);
         p2_sts(xl + xo_bot, O[E - 1][0], O[E - 1][1]);
-      } else if (st_any && q >= zs && q < ze) {
+      } else if (store) {
         // level T: final multiply in scalar, natural x order, one store per row
-        float* const dst = gbase + (int64_t)q * gsz;
 #pragma unroll
         for (int e = 0; e < E; ++e) {
           if (!((st_rows >> e) & 1u)) continue;
           const float4 o = make_float4(coef * p2_lo(O[e][0]), coef * p2_lo(O[e][1]),
                                        coef * p2_hi(O[e][0]), coef * p2_hi(O[e][1]));
           if (st_full4) {
-            *reinterpret_cast<float4*>(dst + (int64_t)e * gsy) = o;
+            *reinterpret_cast<float4*>(gptr + e * gsy) = o;
           } else {
             const float ov[4] = {o.x, o.y, o.z, o.w};
 #pragma unroll
             for (int v = 0; v < V; ++v)
-              if (gx + v < p.L.n0) dst[(int64_t)e * gsy + v] = ov[v];
+              if (gx + v < p.L.n0) gptr[e * gsy + v] = ov[v];
           }
         }
       }
     }
+    gptr += gsz;
     return true;
   };
 

@@ -460,14 +460,21 @@ def test_full_size_jacobi_3d_tiled_equals_plain_and_fp64_error():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("T", [1, 2, 3, 4])
-@pytest.mark.parametrize("E,bx,by", [(4, 16, 16), (4, 8, 32), (4, 32, 8), (2, 16, 16),
-                                     (2, 32, 8), (4, 16, 6)])
+@pytest.mark.parametrize("E,bx,by", [(4, 16, 16), (4, 16, 8), (4, 8, 16), (2, 16, 32),
+                                     (2, 32, 16), (2, 16, 16)])
 def test_packed_stream_kernel_matches_oracle(T, E, bx, by):
     """The packed-FP32 z-streamed kernel (pairs (v0, v2), (v1, v3) in 64-bit
-    registers): bit for bit against the oracle, with n not a multiple of the
-    tile interior, several z segments and a shallower last launch."""
+    registers) in every instantiated block shape: bit for bit against the
+    oracle, with n not a multiple of the tile interior, several z segments
+    and a shallower last launch."""
     g = run_and_check("jacobi-3d", 61, 2 * T + 1, T=T, bx=bx, by=by, bz=1, E=E, kernel="stream")
     assert g.kernel == ots.KERNEL_STREAM
+    with ots.Plan("jacobi-3d", 61, 2 * T + 1, T=T, bx=bx, by=by, bz=1, E=E,
+                  kernel="stream") as plan:
+        assert plan.describe()["Stream Arithmetic"] == "packed-fp32"
+    # shapes without a packed instantiation run the scalar kernel
+    with ots.Plan("jacobi-3d", 61, 5, T=2, bx=32, by=8, bz=1, E=2, kernel="stream") as plan:
+        assert plan.describe()["Stream Arithmetic"] == "scalar"
 
 
 @pytest.mark.gpu
