@@ -77,8 +77,11 @@ __device__ __forceinline__ void p2_lds(const float* a, uint64_t& x, uint64_t& y)
   x = v.x;
   y = v.y;
 }
+// two 8-byte stores: each pair is already an aligned register pair, so no
+// move is needed to assemble a 16-byte (4-register) source
 __device__ __forceinline__ void p2_sts(float* a, uint64_t x, uint64_t y) {
-  *reinterpret_cast<ulonglong2*>(a) = make_ulonglong2(x, y);
+  reinterpret_cast<uint64_t*>(a)[0] = x;
+  reinterpret_cast<uint64_t*>(a)[1] = y;
 }
 // 16 bytes of shared memory in natural order (v0, v1, v2, v3) as the pairs
 // (v0, v2) and (v1, v3)
@@ -188,6 +191,9 @@ __global__ void __launch_bounds__(BX * BY, 1)
       if ((unsigned)(gx + v) < (unsigned)p.L.n0 && (unsigned)(gy + e) < (unsigned)p.L.n1)
         xyin |= 1u << (e * V + v);
   const bool xyall = xyin == ((1u << (E * V)) - 1u);
+  // the zero-ring masking is needed only by warps with a cell outside the
+  // domain in x/y: a warp-uniform flag keeps the common path branch-free
+  const bool warp_xyall = __all_sync(0xffffffffu, xyall);
   // level T stores: this thread's columns in the tile interior; rows whose
   // tile row lies in the interior
   const bool st_x = lx >= HX && lx < HX + rpbx && gx < p.L.n0;
@@ -196,7 +202,9 @@ __global__ void __launch_bounds__(BX * BY, 1)
   for (int e = 0; e < E; ++e)
     if (ly + e >= HY && ly + e < HY + rpby && gy + e < p.L.n1) st_rows |= 1u << e;
   const bool st_any = st_x && st_rows != 0;
-  const bool st_full4 = gx + 3 < p.L.n0;  // all four columns inside (one 16-byte store)
+  // n0 a multiple of 4: every thread's four columns are all inside or all
+  // outside (gx is a multiple of 4), one 16-byte store per row
+  const bool x4 = (p.L.n0 & 3) == 0;
   const int64_t gsz = p.L.sz, gsy = p.L.sy;
   // level T of iteration r writes plane kb + r - T; the pointer walks one
   // plane per iteration and is dereferenced only for planes in [zs, ze)
@@ -304,7 +312,7 @@ __global__ void __launch_bounds__(BX * BY, 1)
           O[e][1] = p2_mul(coef2, O[e][1]);
         }
         const bool zin = (unsigned)q < (unsigned)n2;
-        if (!(zin && xyall)) {  // domain edge: zero the cells outside
+        if (!(zin && warp_xyall)) {  // domain edge: zero the cells outside
 #pragma unroll
           for (int e = 0; e < E; ++e) {
             const unsigned m = zin ? (xyin >> (e * V)) & 0xFu : 0u;
@@ -323,18 +331,22 @@ __global__ void __launch_bounds__(BX * BY, 1)
         p2_sts(xl + xo_bot, O[E - 1][0], O[E - 1][1]);
       } else if (store) {
         // level T: final multiply in scalar, natural x order, one store per row
+        float4 o[E];
 #pragma unroll
-        for (int e = 0; e < E; ++e) {
-          if (!((st_rows >> e) & 1u)) continue;
-          const float4 o = make_float4(coef * p2_lo(O[e][0]), coef * p2_lo(O[e][1]),
-                                       coef * p2_hi(O[e][0]), coef * p2_hi(O[e][1]));
-          if (st_full4) {
-            *reinterpret_cast<float4*>(gptr + e * gsy) = o;
-          } else {
-            const float ov[4] = {o.x, o.y, o.z, o.w};
+        for (int e = 0; e < E; ++e)
+          o[e] = make_float4(coef * p2_lo(O[e][0]), coef * p2_lo(O[e][1]),
+                             coef * p2_hi(O[e][0]), coef * p2_hi(O[e][1]));
+        if (x4) {
+#pragma unroll
+          for (int e = 0; e < E; ++e)
+            if ((st_rows >> e) & 1u) *reinterpret_cast<float4*>(gptr + e * gsy) = o[e];
+        } else {
+#pragma unroll
+          for (int e = 0; e < E; ++e) {
+            const float ov[4] = {o[e].x, o[e].y, o[e].z, o[e].w};
 #pragma unroll
             for (int v = 0; v < V; ++v)
-              if (gx + v < p.L.n0) gptr[e * gsy + v] = ov[v];
+              if (((st_rows >> e) & 1u) && gx + v < p.L.n0) gptr[e * gsy + v] = ov[v];
           }
         }
       }
