@@ -432,8 +432,10 @@ ots_status derive_stream(const ots_plan* pl, int T, StreamCfg* c) {
   c->rpbx = c->tx - 2 * hx;
   c->rpby = c->cy * c->ty - 2 * hy;  // one y halo per cluster tile
   c->shape3p = ots::shape3p_index(c->E, c->bx, c->by);
+  // the packed kernel's branch-free zero ring needs n0 % 4 == 0
   c->packed = p.stream_impl != 1 && c->cy == 1 && T <= ots::kMaxT3p && pl->K &&
-              c->shape3p >= 0 && pl->K->stream3p[T][c->shape3p] != nullptr;
+              pl->geo.real_size % 4 == 0 && c->shape3p >= 0 &&
+              pl->K->stream3p[T][c->shape3p] != nullptr;
   const int maxthr = c->packed ? 512 : (T * c->E >= 8 ? 256 : 512);
   if (c->bx != 8 && c->bx != 16 && c->bx != 32)
     return fail(OTS_ERR_UNSUPPORTED, "stream kernel block x must be 8, 16 or 32 (got %d)", c->bx);

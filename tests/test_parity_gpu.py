@@ -467,20 +467,28 @@ def test_packed_stream_kernel_matches_oracle(T, E, bx, by):
     registers) in every instantiated block shape: bit for bit against the
     oracle, with n not a multiple of the tile interior, several z segments
     and a shallower last launch."""
-    g = run_and_check("jacobi-3d", 61, 2 * T + 1, T=T, bx=bx, by=by, bz=1, E=E, kernel="stream")
-    assert g.kernel == ots.KERNEL_STREAM
-    with ots.Plan("jacobi-3d", 61, 2 * T + 1, T=T, bx=bx, by=by, bz=1, E=E,
-                  kernel="stream") as plan:
-        assert plan.describe()["Stream Arithmetic"] == "packed-fp32"
-    # shapes without a packed instantiation run the scalar kernel
-    with ots.Plan("jacobi-3d", 61, 5, T=2, bx=32, by=8, bz=1, E=2, kernel="stream") as plan:
+    for n in (60, 132):  # several tiles with partial edge tiles, and z segments
+        g = run_and_check("jacobi-3d", n, 2 * T + 1, T=T, bx=bx, by=by, bz=1, E=E,
+                          kernel="stream")
+        assert g.kernel == ots.KERNEL_STREAM
+        with ots.Plan("jacobi-3d", n, 2 * T + 1, T=T, bx=bx, by=by, bz=1, E=E,
+                      kernel="stream") as plan:
+            assert plan.describe()["Stream Arithmetic"] == "packed-fp32"
+    # shapes without a packed instantiation, and n % 4 != 0, run the scalar kernel
+    with ots.Plan("jacobi-3d", 60, 5, T=2, bx=32, by=8, bz=1, E=2, kernel="stream") as plan:
         assert plan.describe()["Stream Arithmetic"] == "scalar"
+    try:
+        with ots.Plan("jacobi-3d", 61, 5, T=T, bx=bx, by=by, bz=1, E=E, kernel="stream") as plan:
+            assert plan.describe()["Stream Arithmetic"] == "scalar"
+    except ots.OtsError as e:  # beyond the scalar kernel's thread limit
+        assert e.status_name == "BLOCK_TOO_LARGE" and bx * by > 256
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n,steps,T,E,bx,by", [(130, 9, 4, 4, 16, 16), (97, 7, 3, 4, 16, 16),
-                                               (64, 8, 4, 2, 16, 16), (33, 5, 2, 4, 8, 8),
-                                               (200, 4, 4, 4, 16, 16), (5, 6, 4, 4, 16, 16)])
+@pytest.mark.parametrize("n,steps,T,E,bx,by", [(132, 9, 4, 4, 16, 16), (96, 7, 3, 4, 16, 16),
+                                               (64, 8, 4, 2, 16, 16), (36, 5, 2, 4, 8, 16),
+                                               (200, 4, 3, 2, 16, 32), (4, 6, 4, 4, 16, 16),
+                                               (97, 7, 3, 4, 16, 16)])
 def test_packed_and_scalar_stream_kernels_agree_bitwise(n, steps, T, E, bx, by):
     """stream_impl 0 (packed) and 1 (scalar) on the same plan shape: identical
     bits, and both equal to the oracle (the reference weight 0.143 too)."""
