@@ -80,9 +80,15 @@ __device__ __forceinline__ uint64_t p2_mul(uint64_t a, uint64_t b) {
   asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
   return d;
 }
-// both halves of a pair ANDed with one 32-bit mask
+// both halves of a pair ANDed with one 32-bit mask (two 32-bit ANDs: no
+// 64-bit mask pair has to be assembled)
 __device__ __forceinline__ uint64_t p2_and(uint64_t a, uint32_t m) {
-  return a & (((uint64_t)m << 32) | (uint64_t)m);
+  uint64_t d;
+  asm("{.reg .b32 l, h; mov.b64 {l, h}, %1; and.b32 l, l, %2; and.b32 h, h, %2;"
+      " mov.b64 %0, {l, h};}"
+      : "=l"(d)
+      : "l"(a), "r"(m));
+  return d;
 }
 // 16 bytes of shared memory as two pairs, and back
 __device__ __forceinline__ void p2_lds(const float* a, uint64_t& x, uint64_t& y) {
