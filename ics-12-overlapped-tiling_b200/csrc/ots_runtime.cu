@@ -1276,15 +1276,20 @@ static ots_status upload_impl(ots_plan* pl, const float* const* state, const flo
   OTS_CUDA(cudaSetDevice(pl->device), "cudaSetDevice");
   for (int f = 0; f < pl->info->ns; ++f) {
     if (!state[f]) return fail(OTS_ERR_INVALID_ARGUMENT, "state field %d is NULL", f);
-    // both ping-pong buffers get the input, as the reference writes it twice:
-    // once from the host, then on the device
     ots_status s = copy_field(pl, pl->state[0][f], state[f], true, pl->geo.padding,
                               pl->geo.padded_size, interior);
     if (s != OTS_OK) return s;
-    OTS_CUDA(cudaMemcpyAsync(pl->state[1][f], pl->state[0][f],
-                             (size_t)pl->field_elems * sizeof(float), cudaMemcpyDeviceToDevice,
-                             pl->stream),
-             "device copy");
+    // Every launch writes every interior cell of its output buffer, so the
+    // second ping-pong buffer's contents are never read before they are
+    // overwritten.  Only phase-limited kernels (-p 1/2/3) stop before their
+    // write-back; for them the second buffer gets the input too, as the
+    // reference writes its input to both buffers
+    // (opencl/jacobi-2d/jacobi-2d.cpp:874-886).
+    if (pl->prm.phase_limit != 0)
+      OTS_CUDA(cudaMemcpyAsync(pl->state[1][f], pl->state[0][f],
+                               (size_t)pl->field_elems * sizeof(float),
+                               cudaMemcpyDeviceToDevice, pl->stream),
+               "device copy");
   }
   for (int a = 0; a < pl->info->na; ++a) {
     if (!aux || !aux[a]) return fail(OTS_ERR_INVALID_ARGUMENT, "aux field %d is NULL", a);
