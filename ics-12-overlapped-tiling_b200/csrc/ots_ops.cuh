@@ -48,8 +48,20 @@ OTS_HD float ots_rsqrt(float v) {
 struct OpArgs {
   float coef;   // averaging weight
   float h2;     // Poisson h^2
-  int variant;  // 0 baseline, 1 reference arithmetic
+  int variant;  // 0 baseline, 1 reference arithmetic, 2 fast division
 };
+
+// Division: IEEE, or in the fast variant CUDA's approximate __fdividef
+// (documented maximum error 2 ulp for |b| in [2^-126, 2^126]); the host
+// (the runner's own -v check) divides exactly.
+OTS_HD float ots_div(float a, float b, bool fast) {
+#if defined(__CUDA_ARCH__)
+  return fast ? __fdividef(a, b) : a / b;
+#else
+  (void)fast;
+  return a / b;
+#endif
+}
 
 OTS_HD float sq(float v) { return v * v; }
 
@@ -228,17 +240,19 @@ struct OpRician2D {
                   sq(c - a(0, 0, dy + 1, dx)) + sq(c - a(0, 0, dy - 1, dx)));
   }
   template <class A>
-  OTS_HD static void apply(const A& a, const float* aux, const OpArgs&, int,
+  OTS_HD static void apply(const A& a, const float* aux, const OpArgs& p, int,
                                                float* o) {
     const float DT = 5.0f, SIGMA2 = 0.0025f, GAMMA = 0.065f / 0.0025f;
+    const bool fast = p.variant == 2;
     float c = a(0, 0, 0, 0), f = aux[0];
-    float r = c * f / SIGMA2;
-    r = (r * (2.38944f + r * (0.950037f + r))) / (4.65314f + r * (2.57541f + r * (1.48937f + r)));
+    float r = ots_div(c * f, SIGMA2, fast);
+    r = ots_div(r * (2.38944f + r * (0.950037f + r)),
+                4.65314f + r * (2.57541f + r * (1.48937f + r)), fast);
     float gl = g_at(a, 0, -1), gr = g_at(a, 0, 1), gt = g_at(a, -1, 0), gb = g_at(a, 1, 0);
     float ugl = a(0, 0, 0, -1) * gl, ugr = a(0, 0, 0, 1) * gr, ugt = a(0, 0, -1, 0) * gt,
           ugb = a(0, 0, 1, 0) * gb;
-    o[0] = (c + DT * (ugb + ugt + ugr + ugl + GAMMA * f * r)) /
-           (1.0f + DT * (gr + gl + gb + gt + GAMMA));
+    o[0] = ots_div(c + DT * (ugb + ugt + ugr + ugl + GAMMA * f * r),
+                   1.0f + DT * (gr + gl + gb + gt + GAMMA), fast);
   }
   // Two-phase form for the overlapped tile, the reference kernel's own order
   // (:271-275 then :292-329): phase 1 stores g once per tile cell, phase 2
@@ -248,17 +262,19 @@ struct OpRician2D {
   template <class A>
   OTS_HD static float phase1(const A& a) { return g_at(a, 0, 0); }
   template <class A, class G>
-  OTS_HD static void apply2(const A& a, const G& g, const float* aux, const OpArgs&, int,
+  OTS_HD static void apply2(const A& a, const G& g, const float* aux, const OpArgs& p, int,
                             float* o) {
     const float DT = 5.0f, SIGMA2 = 0.0025f, GAMMA = 0.065f / 0.0025f;
+    const bool fast = p.variant == 2;
     float c = a(0, 0, 0, 0), f = aux[0];
-    float r = c * f / SIGMA2;
-    r = (r * (2.38944f + r * (0.950037f + r))) / (4.65314f + r * (2.57541f + r * (1.48937f + r)));
+    float r = ots_div(c * f, SIGMA2, fast);
+    r = ots_div(r * (2.38944f + r * (0.950037f + r)),
+                4.65314f + r * (2.57541f + r * (1.48937f + r)), fast);
     float gl = g(0, -1), gr = g(0, 1), gt = g(-1, 0), gb = g(1, 0);
     float ugl = a(0, 0, 0, -1) * gl, ugr = a(0, 0, 0, 1) * gr, ugt = a(0, 0, -1, 0) * gt,
           ugb = a(0, 0, 1, 0) * gb;
-    o[0] = (c + DT * (ugb + ugt + ugr + ugl + GAMMA * f * r)) /
-           (1.0f + DT * (gr + gl + gb + gt + GAMMA));
+    o[0] = ots_div(c + DT * (ugb + ugt + ugr + ugl + GAMMA * f * r),
+                   1.0f + DT * (gr + gl + gb + gt + GAMMA), fast);
   }
 };
 
@@ -268,17 +284,23 @@ struct OpTvUpdate2D {
   static constexpr int DIMS = 2, NS = 1, NA = 2, RX = 1, RY = 1, RZ = 0;
   static constexpr bool STAR = false;
   template <class A>
-  OTS_HD static void apply(const A& a, const float* aux, const OpArgs&, int,
+  OTS_HD static void apply(const A& a, const float* aux, const OpArgs& p, int,
                                                float* o) {
     const float EPI1 = 1e-8f, ALPHA = 1.1f;
+    const bool fast = p.variant == 2;
     float tc = a(0, 0, -1, 0), tr = a(0, 0, -1, 1), ml = a(0, 0, 0, -1), mc = a(0, 0, 0, 0),
           mr = a(0, 0, 0, 1), bl = a(0, 0, 1, -1), bc = a(0, 0, 1, 0);
     float F = aux[0], V = aux[1];
-    float c1 = mc * ots_rsqrt(EPI1 + ((bc - mc) * (bc - mc)) + ((mr - mc) * (mr - mc))) / V;
-    float c2 = mc * ots_rsqrt(EPI1 + ((mc - tc) * (mc - tc)) + ((tr - tc) * (tr - tc))) / V;
-    float c3 = mc * ots_rsqrt(EPI1 + ((bc - mc) * (bc - mc)) + ((mr - mc) * (mr - mc))) / V;
-    float c4 = mc * ots_rsqrt(EPI1 + ((bl - ml) * (bl - ml)) + ((mc - ml) * (mc - ml))) / V;
-    o[0] = 1.0f / (ALPHA + c1 + c2 + c3 + c4) * (ALPHA * F + c1 * bc + c2 * tc + c3 * mr + c4 * ml);
+    float c1 =
+        ots_div(mc * ots_rsqrt(EPI1 + ((bc - mc) * (bc - mc)) + ((mr - mc) * (mr - mc))), V, fast);
+    float c2 =
+        ots_div(mc * ots_rsqrt(EPI1 + ((mc - tc) * (mc - tc)) + ((tr - tc) * (tr - tc))), V, fast);
+    float c3 =
+        ots_div(mc * ots_rsqrt(EPI1 + ((bc - mc) * (bc - mc)) + ((mr - mc) * (mr - mc))), V, fast);
+    float c4 =
+        ots_div(mc * ots_rsqrt(EPI1 + ((bl - ml) * (bl - ml)) + ((mc - ml) * (mc - ml))), V, fast);
+    o[0] = ots_div(1.0f, ALPHA + c1 + c2 + c3 + c4, fast) *
+           (ALPHA * F + c1 * bc + c2 * tc + c3 * mr + c4 * ml);
   }
 };
 
@@ -404,21 +426,34 @@ struct OpCs3D {
     return (float)((double)u * (1.0 / sqrt(1e-9 + (double)a + (double)b + (double)c)) /
                    (double)1.1f);
   }
+  // the fast variant: float 1/sqrt (rsqrt) and approximate division
+  OTS_HD static float cterm_fast(float u, float a, float b, float c) {
+    return ots_div(u * ots_rsqrt(1e-9f + a + b + c), 1.1f, true);
+  }
   template <class A>
-  OTS_HD static void apply(const A& a, const float*, const OpArgs&, int,
+  OTS_HD static void apply(const A& a, const float*, const OpArgs& p, int,
                                                float* o) {
+    const bool fast = p.variant == 2;
     const float ALPHA = 1.1f;
     float u = a(0, 0, 0, 0);
     float zp = a(0, 1, 0, 0), zm = a(0, -1, 0, 0), yp = a(0, 0, 1, 0), ym = a(0, 0, -1, 0),
           xp = a(0, 0, 0, 1), xm = a(0, 0, 0, -1);
     float zm_yp = a(0, -1, 1, 0), zm_xp = a(0, -1, 0, 1), zp_ym = a(0, 1, -1, 0),
           ym_xp = a(0, 0, -1, 1), zp_xm = a(0, 1, 0, -1), yp_xm = a(0, 0, 1, -1);
-    float c1 = cterm(u, sq(zp - u), sq(yp - u), sq(xp - u));
-    float c2 = cterm(u, sq(u - zm), sq(zm_yp - zm), sq(zm_xp - zm));
-    float c3 = cterm(u, sq(zp_ym - ym), sq(u - ym), sq(ym_xp - ym));
-    float c4 = cterm(u, sq(zp_xm - xm), sq(yp_xm - xm), sq(u - xm));
-    o[0] = (ALPHA * u + c1 * (zp + yp + xp) + c2 * zm + c3 * ym + c4 * xm) /
-           (ALPHA + 3.0f * c1 + c2 + c3 + c4);
+    float c1, c2, c3, c4;
+    if (fast) {
+      c1 = cterm_fast(u, sq(zp - u), sq(yp - u), sq(xp - u));
+      c2 = cterm_fast(u, sq(u - zm), sq(zm_yp - zm), sq(zm_xp - zm));
+      c3 = cterm_fast(u, sq(zp_ym - ym), sq(u - ym), sq(ym_xp - ym));
+      c4 = cterm_fast(u, sq(zp_xm - xm), sq(yp_xm - xm), sq(u - xm));
+    } else {
+      c1 = cterm(u, sq(zp - u), sq(yp - u), sq(xp - u));
+      c2 = cterm(u, sq(u - zm), sq(zm_yp - zm), sq(zm_xp - zm));
+      c3 = cterm(u, sq(zp_ym - ym), sq(u - ym), sq(ym_xp - ym));
+      c4 = cterm(u, sq(zp_xm - xm), sq(yp_xm - xm), sq(u - xm));
+    }
+    o[0] = ots_div(ALPHA * u + c1 * (zp + yp + xp) + c2 * zm + c3 * ym + c4 * xm,
+                   ALPHA + 3.0f * c1 + c2 + c3 + c4, fast);
   }
 };
 

@@ -49,7 +49,8 @@ void usage(const char* prog) {
           "      --stencil NAME           Stencil (default: from the program name)\n"
           "      --engine compat|native   Geometry derivation (default compat)\n"
           "      --kernel auto|tile|stream|plain|tex\n"
-          "      --variant ref|baseline   Arithmetic variant (default: ref for compat)\n"
+          "      --variant ref|baseline|fast  Arithmetic variant (default: ref for compat;\n"
+          "                               fast: approximate division, rician / tv / cs-3d)\n"
           "      --coef X                 Averaging weight (Jacobi stencils)\n"
           "      --seed N                 srand seed for the input fill (default 123456)\n"
           "      --init ref|baseline      Inputs: the reference fill everywhere (default), or the\n"
@@ -201,8 +202,12 @@ int main(int argc, char** argv) {
       const std::string k = next();
       p.kernel = k == "tile" ? OTS_KERNEL_TILE : k == "stream" ? OTS_KERNEL_STREAM
                  : k == "plain" ? OTS_KERNEL_PLAIN : k == "tex" ? OTS_KERNEL_TEX : OTS_KERNEL_AUTO;
-    } else if (a == "--variant") p.variant = strcmp(next(), "baseline") == 0 ? OTS_VARIANT_BASELINE : OTS_VARIANT_REF;
-    else if (a == "--coef") p.coef = (float)atof(next());
+    } else if (a == "--variant") {
+      const char* v = next();
+      p.variant = strcmp(v, "baseline") == 0 ? OTS_VARIANT_BASELINE
+                  : strcmp(v, "fast") == 0   ? OTS_VARIANT_FAST
+                                             : OTS_VARIANT_REF;
+    } else if (a == "--coef") p.coef = (float)atof(next());
     else if (a == "--seed") seed = (unsigned)strtoul(next(), nullptr, 10);
     else if (a == "--init") init_baseline = strcmp(next(), "baseline") == 0;
     else if (a == "--plain") plain = true;

@@ -260,8 +260,14 @@ ots_status derive(const ots_params* p, ots_geometry* g, const StencilInfo** info
     return fail(OTS_ERR_INVALID_ARGUMENT, "unknown engine %d", p->engine);
   if (p->kernel < OTS_KERNEL_AUTO || p->kernel > OTS_KERNEL_TEX)
     return fail(OTS_ERR_INVALID_ARGUMENT, "unknown kernel family %d", p->kernel);
-  if (p->variant != OTS_VARIANT_BASELINE && p->variant != OTS_VARIANT_REF)
+  if (p->variant != OTS_VARIANT_BASELINE && p->variant != OTS_VARIANT_REF &&
+      p->variant != OTS_VARIANT_FAST)
     return fail(OTS_ERR_INVALID_ARGUMENT, "unknown variant %d", p->variant);
+  if (p->variant == OTS_VARIANT_FAST && p->stencil != OTS_RICIAN_DENOISE_2D &&
+      p->stencil != OTS_CDSC_TV_UPDATE_2D && p->stencil != OTS_CS_3D)
+    return fail(OTS_ERR_INVALID_ARGUMENT,
+                "the fast-division variant applies to rician-denoise-2d, cdsc-tv-update-2d "
+                "and cs-3d only");
   if (p->phase_limit < 0 || p->phase_limit > 3)
     return fail(OTS_ERR_INVALID_ARGUMENT, "phase limit must be 0..3");
 
@@ -1574,7 +1580,8 @@ ots_status ots_describe(const ots_plan* plan, ots_kv_fn kv, void* user) {
     kv("Stream Arithmetic", plan->scfg.packed ? "packed-fp32" : "scalar", user);
   emit_i("Dynamic Shared Bytes", g.shared_bytes);
   kv("Engine", p.engine == OTS_ENGINE_COMPAT ? "compat" : "native", user);
-  kv("Variant", p.variant == OTS_VARIANT_REF ? "ref" : "baseline", user);
+  kv("Variant", p.variant == OTS_VARIANT_REF ? "ref"
+                : p.variant == OTS_VARIANT_FAST ? "fast" : "baseline", user);
   if (si.r5[0] >= 0) {
     static const char* kR5[] = {"phase2_global_loads", "phase2_shared_loads", "compute_per_point",
                                 "phase3_shared_loads", "phase4_global_stores", "shared_stores",

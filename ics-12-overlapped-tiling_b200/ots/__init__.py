@@ -34,7 +34,7 @@ SID = {n: i for i, n in enumerate(STENCILS)}
 ENGINE_NATIVE, ENGINE_COMPAT = 0, 1
 KERNEL_AUTO, KERNEL_TILE, KERNEL_STREAM, KERNEL_PLAIN, KERNEL_TEX = 0, 1, 2, 3, 4
 KERNELS = {"auto": 0, "tile": 1, "stream": 2, "plain": 3, "tex": 4}
-VARIANT_BASELINE, VARIANT_REF = 0, 1
+VARIANT_BASELINE, VARIANT_REF, VARIANT_FAST = 0, 1, 2
 
 STATUS = {0: "OK", 1: "INVALID_ARGUMENT", 2: "INVALID_GEOMETRY", 3: "SMEM_TOO_LARGE",
           4: "BLOCK_TOO_LARGE", 5: "CUDA", 6: "TIMEOUT", 7: "UNSUPPORTED", 8: "NO_DEVICE",

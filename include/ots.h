@@ -99,8 +99,19 @@ typedef enum ots_kernel {
  * differ.  OTS_VARIANT_BASELINE: jacobi-3d weight 1/7; Poisson as a Jacobi sweep with RHS
  * f and h^2 (5-/7-point); FDTD with the standard Hz sign and the Ey row-0
  * source.  OTS_VARIANT_REF: the reference kernels' arithmetic (0.143f; 8c-sum8 and
- * 26c-sum26; +Ey in the Hz update, no source). */
-typedef enum ots_variant { OTS_VARIANT_BASELINE = 0, OTS_VARIANT_REF = 1 } ots_variant;
+ * 26c-sum26; +Ey in the Hz update, no source).  OTS_VARIANT_FAST (rician-denoise-2d,
+ * cdsc-tv-update-2d, cs-3d only): the baseline arithmetic with every division
+ * replaced by CUDA's approximate division (__fdividef, 2 ulp) and cs-3d's 1/sqrt
+ * terms in float rsqrt -- the latitude the reference's OpenCL build gave its
+ * kernels (default options, single-precision '/' within 2.5 ulp;
+ * opencl/rician-denoise-2d/rician-denoise-2d.cpp:662); results are no longer
+ * bit-reproducible against an IEEE CPU loop, only within the tolerance the
+ * tests state. */
+typedef enum ots_variant {
+  OTS_VARIANT_BASELINE = 0,
+  OTS_VARIANT_REF = 1,
+  OTS_VARIANT_FAST = 2
+} ots_variant;
 
 typedef struct ots_params {
   int32_t stencil;             /* ots_stencil */

@@ -114,7 +114,8 @@ def geometry():
 #     second phase reads E' / g of the cells right of and below the tile,
 #     which no work-item of the tile computes; with one tile those cells are
 #     the zero ring and read as zero;
-#   * cs-3d: variant 2, the first step's y-axis orientation (cs-3d.cpp:259-283).
+#   * cs-3d: oracle variant 9, the first step's y-axis orientation
+#     (cs-3d.cpp:259-283).
 KERNEL_CASES = [
     ("jacobi-3d", 16, 1, 4, 4, 4, 1, 5, 123456, 1),
     ("jacobi-3d", 16, 1, 4, 2, 4, 2, 4, 77, 1),
@@ -124,7 +125,7 @@ KERNEL_CASES = [
     ("poisson-3d", 6, 2, 8, 4, 8, 1, 4, 9, 1),
     ("gradient-3d", 12, 1, 4, 4, 4, 1, 4, 123456, 0),
     ("gradient-3d", 6, 2, 8, 4, 8, 1, 4, 11, 0),
-    ("cs-3d", 12, 1, 4, 4, 4, 1, 4, 123456, 2),
+    ("cs-3d", 12, 1, 4, 4, 4, 1, 4, 123456, 9),
     ("fdtd-2d", 16, 1, 16, 16, 1, 1, 6, 123456, 1),
     ("rician-denoise-2d", 16, 1, 16, 16, 1, 1, 4, 123456, 0),
     ("cdsc-tv-update-2d", 24, 1, 8, 8, 1, 1, 4, 123456, 0),

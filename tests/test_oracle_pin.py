@@ -102,7 +102,7 @@ def test_oracle_matches_reference_generated_kernel(case):
     launch loop).  Bit for bit: jacobi-3d (weight 0.143f), poisson-3d (26c -
     the 26 neighbours), gradient-3d, fdtd-2d (the reference's +Ey, no
     source), rician-denoise-2d, cdsc-tv-update-2d and cs-3d (its first
-    step's y orientation, variant 2), at T = 1 and -- for the 3D star
+    step's y orientation, oracle variant 9), at T = 1 and -- for the 3D star
     stencils -- through the reference's in-tile time step at T = 2."""
     key, fields, aux, want, meta = case
     sid, P, pad, steps, seed, real, T, variant = meta[:8]
@@ -116,21 +116,21 @@ def test_oracle_matches_reference_generated_kernel(case):
 
 
 def test_cs3d_orientation_variants_are_distinct_code_paths():
-    """cs-3d's variant 2 (the reference's first-step y orientation, pinned
-    above) and variant 0 (y+1 as "p1" throughout, the in-tile steps' and the
+    """cs-3d's oracle variant 9 (the reference's first-step y orientation,
+    pinned above) and variant 0 (y+1 as "p1" throughout, the in-tile steps' and the
     engine's) share every operation but the two y-axis neighbours: they agree
     where those neighbours are equal and differ on a generic field."""
     P, pad = 14, 1
     x = O.fill_ref(3, P, pad, P - pad, 3, 1)[0]
     c = O.sweep_f32("cs-3d", [x], steps=1, lo=pad, hi=P - pad, variant=0)[0]
-    d = O.sweep_f32("cs-3d", [x], steps=1, lo=pad, hi=P - pad, variant=2)[0]
+    d = O.sweep_f32("cs-3d", [x], steps=1, lo=pad, hi=P - pad, variant=9)[0]
     assert not np.array_equal(c, d)
     # a field constant along y: the y-axis neighbours equal the centre
     flat = np.ascontiguousarray(np.repeat(x[:, 5:6, :], P, axis=1))
     flat[:, :pad, :] = 0
     flat[:, P - pad:, :] = 0
     e = O.sweep_f32("cs-3d", [flat], steps=1, lo=pad, hi=P - pad, variant=0)[0]
-    f = O.sweep_f32("cs-3d", [flat], steps=1, lo=pad, hi=P - pad, variant=2)[0]
+    f = O.sweep_f32("cs-3d", [flat], steps=1, lo=pad, hi=P - pad, variant=9)[0]
     inner = (slice(pad, P - pad), slice(pad + 1, P - pad - 1), slice(pad, P - pad))
     assert np.array_equal(e[inner], f[inner])
 

@@ -507,3 +507,48 @@ def test_packed_and_scalar_stream_kernels_agree_bitwise(n, steps, T, E, bx, by):
     assert np.array_equal(outs[0].view(np.uint32), want.view(np.uint32))
     run_and_check("jacobi-3d", 45, 6, T=3, bx=16, by=16, bz=1, E=4, kernel="stream",
                   variant=ots.VARIANT_REF)
+
+
+# Fast-division variant (OTS_VARIANT_FAST): __fdividef (2 ulp) and rsqrtf in
+# place of IEEE division / correctly rounded 1/sqrt.  Bound on
+# max |gpu - cpu| / max(|cpu|, 1) against the IEEE FP32 oracle after the step
+# counts used here (relative above 1, absolute below; these stencils' values
+# lie in [0, 1) on the reference fill, so the bound is absolute).
+FAST_TOL = {"rician-denoise-2d": 2e-4, "cdsc-tv-update-2d": 2e-4, "cs-3d": 2e-4}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("st,n,kw", [
+    ("rician-denoise-2d", 130, dict(kernel="tile", T=2, bx=32, by=8, E=4)),
+    ("rician-denoise-2d", 130, dict(kernel="plain")),
+    ("rician-denoise-2d", 130, dict(kernel="stream", T=3, bx=32, by=1, E=1)),
+    ("cdsc-tv-update-2d", 130, dict(kernel="tile", T=3, bx=16, by=16, E=2)),
+    ("cdsc-tv-update-2d", 130, dict(kernel="plain")),
+    ("cs-3d", 44, dict(kernel="tile", T=2, bx=16, by=8, bz=2, E=3)),
+    ("cs-3d", 44, dict(kernel="plain")),
+])
+def test_fast_division_variant_within_tolerance(st, n, kw):
+    steps = 8
+    with ots.Plan(st, n, steps, device=0, variant=ots.VARIANT_FAST, **kw) as plan:
+        assert plan.describe()["Variant"] == "fast"
+        g = plan.geometry
+        state, aux = inputs(plan, 31)
+        plan.upload(state, aux)
+        plan.run()
+        got = plan.download()[0]
+    lo, hi = g.padding, g.padding + g.real_size
+    want = O.sweep_f32(st, state, aux=aux, steps=steps, lo=lo, hi=hi)[0]
+    err = float(np.max(np.abs(got.astype(np.float64) - want) / np.maximum(np.abs(want), 1.0)))
+    assert err <= FAST_TOL[st], (st, kw, err)
+    # against FP64: within a small factor of the IEEE FP32 oracle's own error
+    ref64 = O.sweep_f64(st, state, aux=aux, steps=steps, lo=lo, hi=hi)[0]
+    sl = tuple(slice(lo, hi) for _ in range(g.dims))
+    e_fast = float(np.max(np.abs(got[sl] - ref64[sl])))
+    e_ieee = float(np.max(np.abs(want[sl] - ref64[sl])))
+    assert e_fast <= max(10.0 * e_ieee, FAST_TOL[st]), (e_fast, e_ieee)
+
+
+def test_fast_variant_refused_for_other_stencils():
+    with pytest.raises(ots.OtsError) as ei:
+        ots.derive_geometry(stencil="jacobi-2d", n=64, steps=4, variant=ots.VARIANT_FAST)
+    assert ei.value.status_name == "INVALID_ARGUMENT"
