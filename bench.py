@@ -16,8 +16,15 @@ ranks.
            (--e2e-depth) rotate, so a step's host-to-device copy, the
            previous step's kernels and the one before's device-to-host copy
            run at the same time.
-  plain    the plain one-step-per-launch kernel, same device timing (the
-           comparator of the >= 2x target), reported under "plain".
+  plain    the plain one-step-per-launch kernel, same device timing, and the
+           strongest one-step kernel we have (the z-streamed kernel at T=1
+           in its best block shape): the >= 2x target's comparator is
+           plain.best_one_step (speedup_vs_best_one_step).
+  learned  the learned picker live: the shipped cost model ranks the whole
+           configuration space from geometry alone, the top 10 % (with the
+           plain kernel) are measured, the best is kept; reported with its
+           configuration, how many were measured, and its ratio to the
+           exhaustive-sweep best (value).
   roofline HBM: algorithmic bytes per launch (read + write each cell once,
            8 B x 512^3) / average launch time, against the measured copy
            bandwidth in MEASURED_PEAKS.json.
@@ -379,6 +386,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the live learned pick")
     ap.add_argument("--e2e-depth", type=int, default=3,
                     help="plans in flight in the end-to-end leg (each holds 2 x 537 MB)")
     ap.add_argument("--configs", help="measure the listed workloads (stencil names, comma "
@@ -473,6 +481,7 @@ def main():
     # direction) and the kernels work on three different problems at once
     # (ots_upload_interior_async / ots_run_async / ots_download_interior_async)
     e2e = None
+    latency_ms = None
     if not args.no_e2e:
         depth = max(1, args.e2e_depth)
         plans = [plan] + [ots.Plan(STENCIL, N, STEPS, device=local, **cfg) for _ in range(depth - 1)]
@@ -496,6 +505,16 @@ def main():
             e2e_step(s)
         for pl in plans:
             pl.sync()
+        # latency of one problem alone: upload, 100 steps, download (wall)
+        lat = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            plan.upload_interior_async(host_in, aux_in)
+            plan.run_async(cfg["kernel"])
+            plan.download_interior_async(host_out[0])
+            plan.sync()
+            lat.append(time.perf_counter() - t0)
+        latency_ms = sorted(lat)[1] * 1e3
         barrier(world)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -516,7 +535,30 @@ def main():
                "unit": "GUpdates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "pipeline": "%d plans rotate on their own streams; each step: upload its "
                            "input, 100 steps, download its result (wall clock, all copies in)" % depth,
-               "results_identical_across_plans": bool(same)}
+               "results_identical_across_plans": bool(same),
+               "latency_ms_one_problem": latency_ms,
+               "latency_note": "one problem alone through the same calls: its upload, "
+                               "100 steps and download in sequence (wall clock, median of 3)"}
+
+    # the learned picker live on the same workload (rank 0 measures; the
+    # picker is a host-side tool, not part of the timed job)
+    learned = None
+    if not args.no_learned and rank == 0:
+        try:
+            from ots import model as M
+            from ots import workloads as W
+            with open(os.path.join(ROOT, "ics-12-overlapped-tiling_b200", "ots", "data",
+                                   "cost_model.json")) as fh:
+                cm = M.MLP.from_json(json.load(fh), device=local)
+            best_l, k, size = W.learned_pick(dict(stencil=STENCIL, n=N, steps=STEPS), cm,
+                                             device=local)
+            cm.close()
+            learned = {"gupdates": best_l["gupdates"], "config": W.config_of(best_l),
+                       "measured": k + 1, "space": size,
+                       "over_exhaustive_best": best_l["gupdates"] / (value / world),
+                       "model": "shipped cost model (ots/data/cost_model.json)"}
+        except Exception as e:  # report, never fake
+            learned = {"error": str(e)}
 
     peak, peak_src = peaks()
     bytes_per_launch = BYTES_PER_UPDATE * float(N) ** 3
@@ -552,6 +594,7 @@ def main():
                   "best_one_step": plain_best,
                   "speedup_vs_plain": value / plain_value if plain_value else None,
                   "speedup_vs_best_one_step": value / plain_best if plain_best else None},
+        "learned": learned,
         "gpu_launches": launches_per_step * args.steps,
         "roofline": roofline,
         "cpu_baseline": cpu,

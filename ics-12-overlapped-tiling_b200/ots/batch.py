@@ -6,10 +6,11 @@ runs the batched workload -- 256 independent FP32 grids mixing jacobi-2d,
 poisson-2d (Jacobi sweep with RHS) and gradient-2d, sides log-uniform in
 [64, 2048], step counts uniform in 8..256, inputs uniform [0, 1) -- in two
 single graph launches: tile items with each grid's (T, block, E) picked by the
-learned cost model, and warp items of the y-streamed 2D kernel (T = 4, or the
-grid's step count if smaller); it prints one JSON line with their aggregate
+learned cost model, and warp items of the y-streamed 2D kernel with each
+grid's (T, rows per segment) picked by the cost model (beside it the same
+grids with a fixed T = 4); it prints one JSON line with their aggregate
 GUpdates/s against the same grids run one after another (one launch per step,
-one tile launch per T steps, one streamed launch per T steps).
+one tile launch per T steps, one streamed launch per T steps) and the picks.
 """
 import argparse
 import ctypes
@@ -96,11 +97,35 @@ def pick(grids, cost_model=None, device=0):
     return grids
 
 
-def pick_stream(grids, T=4, rows=1):
-    """Stream-mode choice per grid: T (at most 4, at most the step count) and
-    rows per segment (1 = the library's default)."""
+STREAM_MENU = [dict(T=T, by=rows) for T in range(1, 5) for rows in (1, 16, 32, 64, 128)]
+
+
+def pick_stream(grids, cost_model=None, T=4, rows=1, device=0):
+    """Stream-mode choice per grid.  With a cost model: the best predicted
+    (T, rows per segment) of STREAM_MENU (T 1..4 -- the batch kernel's strip
+    halo covers T <= 4 -- and rows 1 = the library's default, 16 .. 128), from
+    the features of the grid's own y-streamed geometry; without one: T (at
+    most the step count) and `rows`."""
+    from . import model as M
     for g in grids:
-        g.update(kernel="stream", T=max(1, min(T, g["steps"])), bx=32, by=rows, E=1)
+        if cost_model is None:
+            g.update(kernel="stream", T=max(1, min(T, g["steps"])), bx=32, by=rows, E=1)
+            continue
+        feats, cands = [], []
+        for c in STREAM_MENU:
+            if c["T"] > max(1, g["steps"]):
+                continue
+            cfg = dict(kernel="stream", T=c["T"], bx=32, by=c["by"], bz=1, E=1)
+            try:
+                geo = derive_geometry(stencil=g["stencil"], n=g["n"], steps=g["steps"],
+                                      T=c["T"], bx=32, by=c["by"], bz=1, E=1, kernel="stream",
+                                      device=device)
+            except OtsError:
+                continue
+            feats.append(M.features(g["stencil"], cfg, geo))
+            cands.append(c)
+        best = cands[int(cost_model.topk(np.stack(feats), 1)[0])]
+        g.update(kernel="stream", T=best["T"], bx=32, by=best["by"], E=1)
     return grids
 
 
@@ -203,7 +228,8 @@ def main(argv=None):
     grids = pick(workload(a.grids, a.seed), cm)
     ins = inputs(grids)
     if a.mode != "all":
-        one = Batch(pick_stream([dict(g) for g in grids]) if a.mode == "stream-graph" else grids)
+        one = Batch(pick_stream([dict(g) for g in grids], cm) if a.mode == "stream-graph"
+                    else grids)
         for i, (s, x) in enumerate(ins):
             one.upload(i, s, x)
         one.run()  # warm-up
@@ -245,7 +271,21 @@ def main(argv=None):
     tt = sorted(t_tile)[len(t_tile) // 2]
     b.close()
     # the same grids as warp items of the y-streamed kernel
-    sgrids = pick_stream([dict(g) for g in grids])
+    # the streamed batch: per-grid (T, rows) from the cost model, and the same
+    # grids with the fixed choice (T = 4, the library's rows) beside it
+    sgrids = pick_stream([dict(g) for g in grids], cm)
+    fgrids = pick_stream([dict(g) for g in grids])
+    bf = Batch(fgrids)
+    for i, (s, x) in enumerate(ins):
+        bf.upload(i, s, x)
+    bf.run()
+    t_sf = []
+    for _ in range(a.reps):
+        for i, (s, x) in enumerate(ins):
+            bf.upload(i, s, x)
+        t_sf.append(bf.run())
+    bf.close()
+    tsf = sorted(t_sf)[len(t_sf) // 2]
     bs = Batch(sgrids)
 
     def load_s():
@@ -282,6 +322,10 @@ def main(argv=None):
                                     "items": sinfo["items"], "ctas": sinfo["ctas"]},
         "sequential_stream": {"value": upd / tss / 1e9, "seconds": tss},
         "stream_speedup_vs_sequential_plain": t_plain / tsg,
+        "stream_configs_from": "cost model" if cm is not None else "fixed T=4",
+        "stream_graph_fixed_T4": {"value": upd / tsf / 1e9, "seconds": tsf},
+        "stream_picks": [{"stencil": g["stencil"], "n": g["n"], "steps": g["steps"],
+                          "T": g["T"], "rows": g["by"]} for g in sgrids],
     }))
     return 0
 

@@ -241,6 +241,63 @@ def plain_values(records):
             if r.get("kernel") == "plain" and r.get("status") == "ok" and r.get("gupdates", 0) > 0}
 
 
+def workload_records(configs):
+    """The full-size workload sweeps of a bench --configs table (its per-
+    workload 'records'), as dataset records with their stencil and size."""
+    out = []
+    for w in configs.get("workloads", []):
+        for r in w.get("records", []):
+            out.append(dict(r, stencil=w["stencil"], n=w["n"], steps=w["steps"]))
+    return out
+
+
+def leave_one_out_sizes(records, k_frac=0.10, hidden=64, layers=3, epochs=300, seed=0,
+                        device=0):
+    """Leave one stencil out over records of several problem sizes: train on
+    every other stencil's records (all sizes), then for each size of the
+    held-out stencil rank that size's space, measure the top k and the plain
+    kernel (k + 1 = 10 % of the space) and report picked/best per size
+    (keys 'stencil@n')."""
+    by_size = {}
+    for r in records:
+        by_size.setdefault((r["stencil"], int(r.get("n", 0))), []).append(r)
+    report = {}
+    for s in sorted({k[0] for k in by_size}):
+        train = [r for r in records if r["stencil"] != s]
+        X, y, _, _ = dataset(train)
+        if len(X) < 10:
+            continue
+        m = MLP(X.shape[1], hidden, layers, seed=seed, device=device)
+        m.fit(X, y, epochs=epochs, seed=seed)
+        for (st, n), recs in sorted(by_size.items()):
+            if st != s:
+                continue
+            Xs, ys, _, rows = dataset(recs)
+            if len(Xs) < 2:
+                continue
+            actual = np.exp(ys.astype(np.float64))
+            p = plain_values(recs).get(s, 0.0)
+            space = len(Xs) + (1 if p else 0)
+            k = max(1, int(math.floor(k_frac * space)) - (1 if p else 0))
+            top = m.topk(Xs, k)
+            picked = max(float(np.max(actual[top])), p)
+            best = max(float(np.max(actual)), p)
+            report["%s@%d" % (s, n)] = {
+                "space": space, "k": k, "measure_cost": (k + (1 if p else 0)) / float(space),
+                "picked_over_best": picked / best, "picked_gupdates": picked,
+                "best_gupdates": best,
+                "top1_over_best": max(float(actual[top[0]]), p) / best,
+                "random_k_over_best": expected_best_of_random(np.maximum(actual, p), k) / best,
+                "picked_config": {q: rows[int(top[int(np.argmax(actual[top]))])][q]
+                                  for q in ("kernel", "T", "bx", "by", "bz", "E")}}
+        m.close()
+    if report:
+        report["_mean"] = {q: float(np.mean([v[q] for v in report.values()]))
+                           for q in ("picked_over_best", "top1_over_best", "random_k_over_best",
+                                     "measure_cost")}
+    return report
+
+
 def leave_one_out(records, k_frac=0.10, hidden=64, layers=3, epochs=300, batch=128, lr=3e-3,
                   weight_decay=1e-4, seed=0, device=0, held_out=None):
     """Train without stencil s, rank s's space, measure the top k -- and the

@@ -2,6 +2,7 @@
 the shipped model.
 
     python -m ots.picker --data ots/data/sweeps_b200.json --report report.json \
+        [--extra ots/data/configs_b200.json --report-sizes sizes.json] \
         [--save-model ots/data/cost_model.json]
 
 For each held-out stencil: train the MLP on every other stencil's measured
@@ -29,9 +30,27 @@ def main(argv=None):
     ap.add_argument("--layers", type=int, default=3)
     ap.add_argument("--k-frac", type=float, default=0.10)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--extra", help="a bench --configs table: its full-size workload sweeps "
+                    "join the training data, and picks are also reported per size")
+    ap.add_argument("--report-sizes", help="write the per-size leave-one-out report here")
     a = ap.parse_args(argv)
-    recs = json.load(open(a.data))["records"]
-    rep = model.leave_one_out(recs, k_frac=a.k_frac, hidden=a.hidden, layers=a.layers,
+    base = json.load(open(a.data))["records"]
+    recs = base
+    if a.extra:
+        full = model.workload_records(json.load(open(a.extra)))
+        recs = base + full
+        if a.report_sizes:
+            rs = model.leave_one_out_sizes(recs, k_frac=a.k_frac, hidden=a.hidden,
+                                           layers=a.layers, epochs=a.epochs, seed=a.seed)
+            for s, r in sorted(rs.items()):
+                if s != "_mean":
+                    print("%-26s space=%4d k=%3d picked/best=%.3f top1/best=%.3f "
+                          "random-k/best=%.3f" % (s, r["space"], r["k"], r["picked_over_best"],
+                                                  r["top1_over_best"], r["random_k_over_best"]))
+            with open(a.report_sizes, "w") as fh:
+                json.dump(rs, fh, indent=1)
+    # the per-stencil report ranks one problem size's space (the sweep's)
+    rep = model.leave_one_out(base, k_frac=a.k_frac, hidden=a.hidden, layers=a.layers,
                               epochs=a.epochs, seed=a.seed)
     for s, r in sorted(rep.items()):
         if s == "_mean":

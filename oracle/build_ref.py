@@ -234,6 +234,21 @@ def build_kernel_case(stencil, n, T, bx, by, bz, E, steps, cxx="g++"):
     return lib
 
 
+# The reference's own CUDA Jacobi-2D runner (cuda/jacobi-2d/jacobi-2d.cu),
+# built at T = 1 (its jacobi_2d_kernel_notimetiling, :88-105) for sm_100a: a
+# GPU data point of the reference beside the engine's kernels.
+CUDA_JACOBI2D = os.path.join(OUT, "ref_cuda_jacobi2d")
+
+
+def build_cuda_jacobi2d(ref_root, nvcc="nvcc"):
+    src = os.path.join(ref_root, "cuda", "jacobi-2d", "jacobi-2d.cu")
+    if not os.path.exists(src):
+        return False
+    subprocess.check_call([nvcc, "-O3", "-gencode", "arch=compute_100a,code=sm_100a",
+                           "-DTIME_TILE_SIZE=1", "-w", src, "-o", CUDA_JACOBI2D])
+    return True
+
+
 def build(ref_root=None, cxx="g++", verbose=False):
     ref_root = ref_root or os.environ.get("OTS_REFERENCE_DIR", "/root/reference")
     if not os.path.isdir(os.path.join(ref_root, "opencl")):
@@ -248,6 +263,11 @@ def build(ref_root=None, cxx="g++", verbose=False):
             fh.write(body)
     gen_geometry_and_fill(ref_root)
     gen_generators(ref_root, cxx)
+    try:
+        build_cuda_jacobi2d(ref_root)
+    except (OSError, subprocess.CalledProcessError) as e:  # optional data point
+        if verbose:
+            print("build_ref: reference CUDA jacobi-2d not built:", e)
     lib = os.path.join(OUT, "libots_ref.so")
     cmd = [cxx, "-O2", "-g", "-fPIC", "-shared", "-I", OUT, "-I", HERE,
            os.path.join(HERE, "ref_harness.cpp"), os.path.join(OUT, "ref_gen.cpp"), "-o", lib]

@@ -144,3 +144,29 @@ def test_batched_stream_rejects_mixed_and_deep_grids():
     with pytest.raises(OtsError) as ei:
         B.Batch([dict(stencil="jacobi-2d", n=64, steps=8, T=6, kernel="stream")])
     assert ei.value.status_name == "UNSUPPORTED"
+
+
+@pytest.mark.gpu
+def test_cost_model_picks_stream_shapes_per_grid_and_batch_matches_oracle():
+    """The streamed batch with per-grid (T, rows per segment) from the
+    shipped cost model: every pick is a valid menu entry within the grid's
+    step count, and the one-launch result equals each grid's oracle run."""
+    import json
+    import os
+    from ots import model as M
+    path = os.path.join(os.path.dirname(B.__file__), "data", "cost_model.json")
+    cm = M.MLP.from_json(json.load(open(path)))
+    grids = [dict(g) for g in STREAM_GRIDS]
+    B.pick_stream(grids, cm)
+    for g in grids:
+        assert g["kernel"] == "stream" and 1 <= g["T"] <= 4 and g["T"] <= max(1, g["steps"])
+        assert g["by"] in (1, 16, 32, 64, 128)
+    b = B.Batch(grids)
+    ins = B.inputs(grids, seed=9)
+    for i, (s, a) in enumerate(ins):
+        b.upload(i, s, a)
+    b.run()
+    for i, (g, (s, a)) in enumerate(zip(grids, ins)):
+        check_same(g, b.download(i), oracle_run(g, s, a))
+    b.close()
+    cm.close()
