@@ -39,6 +39,10 @@ constexpr int kMaxTg = 6;  // generic 2D stream kernel levels
 using Stream1dLaunch = cudaError_t (*)(const Stream1dParams&, dim3, cudaStream_t);
 constexpr int kStream1dVs[3] = {4, 8, 16};  // cells per lane of the 1D register kernel
 using Occ2dFn = cudaError_t (*)(int*);
+// the generic 2D stream kernels: `fast` selects the fast-division
+// instantiation where an op has one (Rician)
+using Occ2dgFn = cudaError_t (*)(int*, bool fast);
+using Attr2dgFn = cudaError_t (*)(cudaFuncAttributes*, bool fast);
 // stream kernel queries take the cluster flag (the clustered instantiation)
 using StreamAttrFn = cudaError_t (*)(cudaFuncAttributes*, bool);
 using StreamOccFn = cudaError_t (*)(int*, int, size_t, bool);
@@ -65,8 +69,8 @@ struct StencilKernels {
   AttrFn stream2d_attr[kMaxT + 1] = {};
   Occ2dFn stream2d_occ[kMaxT + 1] = {};
   Stream2dgLaunch stream2dg[kMaxTg + 1] = {};  // [T], any 2D stencil through apply()
-  AttrFn stream2dg_attr[kMaxTg + 1] = {};
-  Occ2dFn stream2dg_occ[kMaxTg + 1] = {};
+  Attr2dgFn stream2dg_attr[kMaxTg + 1] = {};
+  Occ2dgFn stream2dg_occ[kMaxTg + 1] = {};
   Stream1dLaunch stream1d[3] = {};  // [index of V in kStream1dVs]
   AttrFn stream1d_attr[3] = {};
 };
@@ -227,9 +231,12 @@ void fill_stream3p_shape(StencilKernels& k, std::integer_sequence<int, Ts...>) {
    ...);
 }
 
-// Defined in ots_k_jacobi_3d_p<N>.cu: the packed kernel's table entries.
+// Defined in ots_k_{jacobi,poisson}_3d_p<N>.cu: the packed kernel's table
+// entries.
 void fill_stream3p_jacobi_3d_a(StencilKernels& k);
 void fill_stream3p_jacobi_3d_b(StencilKernels& k);
+void fill_stream3p_poisson_3d_a(StencilKernels& k);
+void fill_stream3p_poisson_3d_b(StencilKernels& k);
 
 template <class Op, int EAX, int... Es>
 void fill_tile(StencilKernels& k, std::integer_sequence<int, Es...>) {
@@ -265,28 +272,34 @@ cudaError_t attr_stream1d(cudaFuncAttributes* a) {
 }
 
 // The y-streamed kernel of a stencil without the five-point form: FDTD-2D
-// has its own two-phase kernel; every other op goes through its apply().
+// and Rician-denoise-2D have their own two-phase kernels (Rician's in two
+// instantiations, IEEE and fast division: `fast` picks one); every other op
+// goes through its apply().
 template <class Op, int T>
-constexpr auto stream2dg_entry() {
+auto stream2dg_entry(bool fast = false) {
+  (void)fast;
   if constexpr (std::is_same_v<Op, OpFdtd2D>)
     return &stream2d_fdtd_kernel<T>;
+  else if constexpr (std::is_same_v<Op, OpRician2D>)
+    return fast ? &stream2d_rician_kernel<T, true> : &stream2d_rician_kernel<T, false>;
   else
     return &stream2dg_kernel<Op, T>;
 }
 
 template <class Op, int T>
 cudaError_t launch_stream2dg(const Stream2dgParams& p, dim3 g, cudaStream_t s) {
-  return launch_k(stream2dg_entry<Op, T>(), g, dim3(kStream2dThreads), 0, s, 1, p);
+  return launch_k(stream2dg_entry<Op, T>(p.op.variant == 2), g, dim3(kStream2dThreads), 0, s, 1,
+                  p);
 }
 
 template <class Op, int T>
-cudaError_t attr_stream2dg(cudaFuncAttributes* a) {
-  return cudaFuncGetAttributes(a, stream2dg_entry<Op, T>());
+cudaError_t attr_stream2dg(cudaFuncAttributes* a, bool fast) {
+  return cudaFuncGetAttributes(a, stream2dg_entry<Op, T>(fast));
 }
 
 template <class Op, int T>
-cudaError_t occ_stream2dg(int* blocks) {
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, stream2dg_entry<Op, T>(),
+cudaError_t occ_stream2dg(int* blocks, bool fast) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, stream2dg_entry<Op, T>(fast),
                                                        kStream2dThreads, 0);
 }
 

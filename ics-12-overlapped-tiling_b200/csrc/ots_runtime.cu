@@ -402,8 +402,13 @@ ots_status derive_stream2d(const ots_plan* pl, int T, Stream2dCfg* c) {
   const int n = pl->geo.real_size;
   c->ntx = ceil_div(n, c->rpbx);
   int blocks = 0;
-  auto occ = c->generic ? pl->K->stream2dg_occ[T] : pl->K->stream2d_occ[T];
-  if (!occ || occ(&blocks) != cudaSuccess || blocks < 1) blocks = 1;
+  const bool fast = pl->prm.variant == OTS_VARIANT_FAST;
+  cudaError_t oe = cudaErrorInvalidValue;
+  if (c->generic && pl->K->stream2dg_occ[T])
+    oe = pl->K->stream2dg_occ[T](&blocks, fast);
+  else if (!c->generic && pl->K->stream2d_occ[T])
+    oe = pl->K->stream2d_occ[T](&blocks);
+  if (oe != cudaSuccess || blocks < 1) blocks = 1;
   c->warps_per_sm = blocks * (ots::kStream2dThreads / 32);
   c->zseg = ots::stream2d_zseg(n, c->R * T, c->ntx, pl->sm_count, c->warps_per_sm);
   // block_y > 1 sets the rows per segment directly (tuning); else the model
@@ -459,7 +464,7 @@ ots_status derive_stream(const ots_plan* pl, int T, StreamCfg* c) {
     return fail(OTS_ERR_INVALID_GEOMETRY,
                 "Consistency error! stream tile %d x %d leaves no interior at T=%d", c->tx, c->ty,
                 T);
-  c->smem = c->packed ? ots::stream3p_smem_bytes(T, c->tx, c->ty, c->by) + 128
+  c->smem = c->packed ? ots::stream3p_smem_bytes(T, c->tx, c->ty, c->by, pl->info->na) + 128
                       : ots::stream_smem_bytes(T, c->tx, c->ty, c->cy, pl->info->na);
   if (c->smem > pl->smem_optin)
     return fail(OTS_ERR_SMEM_TOO_LARGE,
@@ -665,8 +670,14 @@ void fill_geometry_for_kernel(ots_plan* pl) {
       g.useful_ratio = (n * n) / ((double)ots::kStream2dWidth * c.ntx * c.nseg *
                                   (double)(c.zseg + 2 * c.R * c.T));
     }
-    auto attr = c.generic ? pl->K->stream2dg_attr[c.T] : pl->K->stream2d_attr[c.T];
-    if (attr && attr(&a) == cudaSuccess) g.registers = a.numRegs;
+    if (c.generic) {
+      auto attr = pl->K->stream2dg_attr[c.T];
+      if (attr && attr(&a, pl->prm.variant == OTS_VARIANT_FAST) == cudaSuccess)
+        g.registers = a.numRegs;
+    } else {
+      auto attr = pl->K->stream2d_attr[c.T];
+      if (attr && attr(&a) == cudaSuccess) g.registers = a.numRegs;
+    }
     g.ctas_per_sm = c.warps_per_sm / (ots::kStream2dThreads / 32);
   } else if (g.kernel == OTS_KERNEL_STREAM) {
     const StreamCfg& c = pl->scfg;

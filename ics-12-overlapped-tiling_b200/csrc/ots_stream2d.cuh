@@ -559,4 +559,176 @@ __global__ void __launch_bounds__(kStream2dThreads)
   if (r < nit) step(PhaseG<0>{}, r);
 }
 
+// Rician-denoise-2D streamed in its two phases.  The fused update
+// (OpRician2D::apply) recomputes g = 1/sqrt(eps + |grad u|^2) at the four
+// neighbours of every cell, four rsqrt and ~200 more instructions per update;
+// here every level computes g once per cell, one row ahead of its update, the
+// order of the reference kernel (opencl/rician-denoise-2d/rician-denoise-2d.cpp:
+// 271-275 then :292-329) and of the two-phase tile step.  The operations and
+// their operands are those of OpRician2D::g_at and ::apply2, so the result is
+// bit for bit the fused kernels'.
+//
+// Level t works on row q = k - 2t (the update reaches two rows: g of the rows
+// beside q needs u two rows away).  At iteration k it first computes
+// g_{t-1}(q + 1) from u_{t-1} rows q .. q + 2 -- row q + 2 is what level t-1
+// produced this iteration -- then updates row q from u_{t-1} rows q - 1 .. q + 1,
+// g_{t-1} rows q - 1 .. q + 1 and F(q).  Each level keeps the four newest rows
+// of its u and of the g computed from them in registers, in slots that rotate
+// with the iteration index (4 phases), so no row is copied.  Level t's F row
+// for the next iteration is fetched as soon as this iteration's is used.
+// FAST selects the division (ots_div): a template argument, so the kernel of
+// one variant carries no code of the other.
+template <int N>
+struct PhaseR {
+  static constexpr int value = N;
+};
+
+template <int T, bool FAST>
+__global__ void __launch_bounds__(kStream2dThreads)
+    stream2d_rician_kernel(const __grid_constant__ Stream2dgParams p) {
+  constexpr int V = 4, R = 2, HX = (R * T + 3) / 4 * 4;
+  constexpr int RPBX = kStream2dWidth - 2 * HX;
+  static_assert(RPBX >= 4, "depth");
+  constexpr float DT = 5.0f, SIGMA2 = 0.0025f, GAMMA = 0.065f / 0.0025f;
+  grid_dependency_sync();
+  const int w = blockIdx.x * (kStream2dThreads / 32) + (threadIdx.x >> 5);
+  if (w >= p.ntx * p.nseg) return;  // whole warps only
+  const int strip = w % p.ntx, seg = w / p.ntx;
+  const int lane = threadIdx.x & 31;
+  const int nx = p.L.n0, ny = p.L.n1;
+  const int64_t sy = p.L.sy;
+  const int gx = strip * RPBX - HX + V * lane;  // multiple of 4
+  unsigned xin = 0;
+#pragma unroll
+  for (int v = 0; v < V; ++v)
+    if ((unsigned)(gx + v) < (unsigned)nx) xin |= 1u << v;
+  const bool xall = xin == 0xFu;
+  const bool wx = V * lane >= HX && V * lane < HX + RPBX;
+  const int ys = seg * p.zseg;
+  const int ye = min(ny, ys + p.zseg);
+  const int kb = ys - R * T;
+  const int nit = (ye + R * T - 1) - kb + 1;
+  constexpr bool fast = FAST;
+  const float* const F = p.aux[0];
+
+  auto load4 = [&](const float* base, int k, float (&d)[V]) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) d[v] = 0.0f;
+    if ((unsigned)k < (unsigned)ny) {
+      const float* src = base + (int64_t)k * sy + gx;
+      if (xall) {
+        const float4 a = __ldg(reinterpret_cast<const float4*>(src));
+        d[0] = a.x; d[1] = a.y; d[2] = a.z; d[3] = a.w;
+      } else {
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+          if ((xin >> v) & 1) d[v] = __ldg(src + v);
+      }
+    }
+  };
+
+  // U[t][s]: level t's rows (t = 0: the input), newest in slot (iteration % 4)
+  // G[t][s]: g of level t's rows, g(row) in the slot of the iteration that
+  // computed it (one iteration after the row itself)
+  float U[T][4][V], G[T][4][V];
+  float Pf[2][V];  // input rows fetched ahead
+  float Ff[T][V];  // level t + 1's F row of the coming iteration
+#pragma unroll
+  for (int t = 0; t < T; ++t)
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+#pragma unroll
+      for (int v = 0; v < V; ++v) U[t][s][v] = G[t][s][v] = 0.0f;
+  load4(p.in[0], kb, Pf[0]);
+  load4(p.in[0], kb + 1, Pf[1]);
+#pragma unroll
+  for (int t = 1; t <= T; ++t) load4(F, kb - R * t, Ff[t - 1]);
+
+  auto step = [&](auto ph, int r) {
+    constexpr int PH = decltype(ph)::value;
+    constexpr int S0 = PH, S1 = (PH + 3) & 3, S2 = (PH + 2) & 3, S3 = (PH + 1) & 3;  // age 0..3
+    const int k = kb + r;
+#pragma unroll
+    for (int v = 0; v < V; ++v) U[0][S0][v] = Pf[PH & 1][v];
+    load4(p.in[0], k + 2, Pf[PH & 1]);
+#pragma unroll
+    for (int t = 1; t <= T; ++t) {
+      const int q = k - R * t;
+      // u_{t-1}: rows q+2 (age 0), q+1 (1), q (2), q-1 (3)
+      const float(&up2)[V] = U[t - 1][S0];
+      const float(&up1)[V] = U[t - 1][S1];
+      const float(&u0)[V] = U[t - 1][S2];
+      const float(&um1)[V] = U[t - 1][S3];
+      // phase 1: g_{t-1}(q + 1) (OpRician2D::g_at at row q + 1)
+      {
+        const float l = __shfl_up_sync(0xffffffffu, up1[V - 1], 1);
+        const float rr = __shfl_down_sync(0xffffffffu, up1[0], 1);
+        const bool rin = (unsigned)(q + 1) < (unsigned)ny;
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          const float c = up1[v];
+          const float xp = v < V - 1 ? up1[v + 1] : rr;
+          const float xm = v > 0 ? up1[v - 1] : l;
+          const float g = ots_rsqrt(1.0E-20f + sq(c - xp) + sq(c - xm) + sq(c - up2[v]) +
+                                    sq(c - u0[v]));
+          G[t - 1][S0][v] = (rin && ((xin >> v) & 1)) ? g : 0.0f;
+        }
+      }
+      // g_{t-1}: rows q+1 (slot S0, just computed), q (S1), q-1 (S2)
+      const float(&gb)[V] = G[t - 1][S0];
+      const float(&gc)[V] = G[t - 1][S1];
+      const float(&gtp)[V] = G[t - 1][S2];
+      // phase 2: the update of row q (OpRician2D::apply2)
+      const float(&fq)[V] = Ff[t - 1];
+      const float ul = __shfl_up_sync(0xffffffffu, u0[V - 1], 1);
+      const float ur = __shfl_down_sync(0xffffffffu, u0[0], 1);
+      const float gl_ = __shfl_up_sync(0xffffffffu, gc[V - 1], 1);
+      const float gr_ = __shfl_down_sync(0xffffffffu, gc[0], 1);
+      const bool qin = (unsigned)q < (unsigned)ny;
+      float o[V];
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const float c = u0[v], f = fq[v];
+        float rv = ots_div(c * f, SIGMA2, fast);
+        rv = ots_div(rv * (2.38944f + rv * (0.950037f + rv)),
+                     4.65314f + rv * (2.57541f + rv * (1.48937f + rv)), fast);
+        const float gl = v > 0 ? gc[v - 1] : gl_;
+        const float gr = v < V - 1 ? gc[v + 1] : gr_;
+        const float gt = gtp[v], g_b = gb[v];
+        const float ugl = (v > 0 ? u0[v - 1] : ul) * gl;
+        const float ugr = (v < V - 1 ? u0[v + 1] : ur) * gr;
+        const float ugt = um1[v] * gt, ugb = up1[v] * g_b;
+        const float res = ots_div(c + DT * (ugb + ugt + ugr + ugl + GAMMA * f * rv),
+                                  1.0f + DT * (gr + gl + g_b + gt + GAMMA), fast);
+        o[v] = (qin && ((xin >> v) & 1)) ? res : 0.0f;
+      }
+      load4(F, q + 1, Ff[t - 1]);
+      if (t < T) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) U[t][S0][v] = o[v];
+      } else if (q >= ys && q < ye && wx) {
+        float* dst = p.out[0] + (int64_t)q * sy + gx;
+        if (xall) {
+          *reinterpret_cast<float4*>(dst) = make_float4(o[0], o[1], o[2], o[3]);
+        } else {
+#pragma unroll
+          for (int v = 0; v < V; ++v)
+            if ((xin >> v) & 1) dst[v] = o[v];
+        }
+      }
+    }
+  };
+
+  int r = 0;
+  for (; r + 3 < nit; r += 4) {
+    step(PhaseR<0>{}, r);
+    step(PhaseR<1>{}, r + 1);
+    step(PhaseR<2>{}, r + 2);
+    step(PhaseR<3>{}, r + 3);
+  }
+  if (r < nit) step(PhaseR<0>{}, r++);
+  if (r < nit) step(PhaseR<1>{}, r++);
+  if (r < nit) step(PhaseR<2>{}, r++);
+}
+
 }  // namespace ots

@@ -1,5 +1,6 @@
 // ots_stream3p.cuh -- z-streamed overlapped time tile for the 3D seven-point
-// Jacobi stencil with packed FP32 arithmetic.
+// stencils (Jacobi-3D, and Poisson-3D in its star form) with packed FP32
+// arithmetic.
 //
 // Same scheme and results as stream_kernel (ots_stream.cuh): a CTA owns an
 // x/y tile (4 x-cells and E rows per thread, halos of round4(T) columns and T
@@ -39,6 +40,13 @@
 // level ANDs the bits of every pair of row e with one 32-bit mask, all ones or
 // zero: (plane inside) ? rowmask[e] : 0.  A cleared pair is +0.0 exactly.
 //
+// Poisson-3D reads its right-hand side f: level t needs f of plane k - t, so
+// f streams through a ring of its own (T + 2 planes, TMA, one mbarrier each),
+// like the scalar kernel's; its update is (s - h^2 f) / 6 as
+// s + (-h^2) f, which is bit for bit s - h^2 f (negation is exact and
+// round-to-nearest is symmetric), times 1/6; the product passes through the
+// zero-ring AND before the add, so the two never fuse into one rounding.
+//
 // Every mbarrier wait is bounded (p.wait_ns); on a timeout the CTA records
 // the error word, drains its own copies still in flight (bounded by time
 // only) and all its threads leave together.
@@ -47,6 +55,8 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <type_traits>
 
 #include "ots_stream.cuh"
 
@@ -127,7 +137,8 @@ inline int shape3p_index(int E, int BX, int BY) {
 //   NST ring stages of TX x TY floats (the TMA boxes),
 //   exchange rows: levels 1 .. T-1, 2 parities, BY thread rows, 2 rows (the
 //   thread row's first and last, pair order), TX floats each,
-//   NST mbarriers.
+//   ops with an aux field: T + 2 f stages (TX x TY floats each),
+//   NST mbarriers, then one per f stage.
 // NST is 8 where that fits the 227 KB a CTA may use, else 4.
 constexpr size_t kSmemPerCta = 227 * 1024;
 __host__ __device__ constexpr size_t stream3p_stage_floats(int TX, int TY) {
@@ -136,15 +147,19 @@ __host__ __device__ constexpr size_t stream3p_stage_floats(int TX, int TY) {
 __host__ __device__ constexpr size_t stream3p_xbuf_floats(int T, int TX, int BY) {
   return (size_t)(T > 1 ? T - 1 : 0) * 2 * BY * 2 * TX;
 }
-__host__ __device__ constexpr size_t stream3p_bytes(int nst, int T, int TX, int TY, int BY) {
-  return ((size_t)nst * stream3p_stage_floats(TX, TY) + stream3p_xbuf_floats(T, TX, BY)) * 4 +
-         (size_t)nst * 8;
+__host__ __device__ constexpr int stream3p_aux_stages(int T, int na) { return na > 0 ? T + 2 : 0; }
+__host__ __device__ constexpr size_t stream3p_bytes(int nst, int T, int TX, int TY, int BY,
+                                                    int na) {
+  return ((size_t)(nst + stream3p_aux_stages(T, na)) * stream3p_stage_floats(TX, TY) +
+          stream3p_xbuf_floats(T, TX, BY)) * 4 +
+         (size_t)(nst + stream3p_aux_stages(T, na)) * 8;
 }
-__host__ __device__ constexpr int stream3p_stages(int T, int TX, int TY, int BY) {
-  return stream3p_bytes(8, T, TX, TY, BY) <= kSmemPerCta ? 8 : 4;
+__host__ __device__ constexpr int stream3p_stages(int T, int TX, int TY, int BY, int na) {
+  return stream3p_bytes(8, T, TX, TY, BY, na) <= kSmemPerCta ? 8 : 4;
 }
-__host__ __device__ constexpr size_t stream3p_smem_bytes(int T, int TX, int TY, int BY) {
-  return stream3p_bytes(stream3p_stages(T, TX, TY, BY), T, TX, TY, BY);
+__host__ __device__ constexpr size_t stream3p_smem_bytes(int T, int TX, int TY, int BY,
+                                                         int na) {
+  return stream3p_bytes(stream3p_stages(T, TX, TY, BY, na), T, TX, TY, BY, na);
 }
 
 // Warps hold whole thread rows (BX = 8, 16 or 32), so the x neighbours a
@@ -157,16 +172,22 @@ __global__ void __launch_bounds__(BX * BY, 1)
   constexpr int V = 4;
   constexpr int HX = StreamGeom<T>::HX, HY = StreamGeom<T>::HY;
   constexpr int TX = V * BX, TY = E * BY;
-  constexpr int NST = stream3p_stages(T, TX, TY, BY), LA = NST - 2;
+  constexpr bool FR = Op::NA > 0;  // f ring (Poisson-3D)
+  constexpr int NF = stream3p_aux_stages(T, Op::NA);
+  constexpr int NST = stream3p_stages(T, TX, TY, BY, Op::NA), LA = NST - 2;
   constexpr int PL = (int)stream3p_stage_floats(TX, TY);  // floats per stage
   constexpr int XS = BY * 2 * TX;                          // floats per exchange buffer
   constexpr int rpbx = TX - 2 * HX, rpby = TY - 2 * HY;
   constexpr unsigned box_bytes = (unsigned)(TX * TY) * sizeof(float);
   static_assert(BX == 8 || BX == 16 || BX == 32, "a warp holds whole thread rows");
   static_assert(rpbx >= 4 && rpby >= 1, "the tile keeps an interior");
+  static_assert(std::is_same_v<Op, OpJacobi3D> || std::is_same_v<Op, OpPoisson3D>,
+                "the packed arithmetic is written for these two ops");
   extern __shared__ __align__(128) float smem[];
   float* const xbase = smem + NST * PL;  // exchange buffers
-  uint64_t* const bars = reinterpret_cast<uint64_t*>(xbase + (T > 1 ? (T - 1) * 2 * XS : 0));
+  float* const fbase = xbase + (T > 1 ? (T - 1) * 2 * XS : 0);  // f stages
+  uint64_t* const bars = reinterpret_cast<uint64_t*>(fbase + NF * PL);
+  uint64_t* const fbars = bars + NST;
   const int tid = threadIdx.x + BX * threadIdx.y;
   const int n2 = p.L.n2;
   grid_dependency_sync();
@@ -186,7 +207,7 @@ __global__ void __launch_bounds__(BX * BY, 1)
   const int xo_below = ((ty + 1 < BY ? ty + 1 : ty) * 2 + 0) * TX + lx;
 
   if (tid == 0) {
-    for (int s = 0; s < NST; ++s) mbar_init(&bars[s], 1);
+    for (int s = 0; s < NST + NF; ++s) mbar_init(&bars[s], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
@@ -227,8 +248,10 @@ __global__ void __launch_bounds__(BX * BY, 1)
   // plane per iteration and is dereferenced only for planes in [zs, ze)
   // (where gx, gy and the plane index are all inside the array)
   float* gptr = p.out + (int64_t)gy * gsy + gx + (int64_t)(kb - T) * gsz;
-  const uint64_t coef2 = p2_make(p.op.coef, p.op.coef);
-  const float coef = p.op.coef;
+  // Jacobi: coef * sum; Poisson: (sum + (-h^2) f) * (1/6)
+  const float coef = FR ? 1.0f / 6.0f : p.op.coef;
+  const uint64_t coef2 = p2_make(coef, coef);
+  const uint64_t nh2 = p2_make(-p.op.h2, -p.op.h2);
   const int zlo = zs + T, zhi = ze + T;  // iterations' k range whose level-T plane is stored
 
   // test hook: CTA 0 arms the stage of running plane hold_plane but never
@@ -239,6 +262,10 @@ __global__ void __launch_bounds__(BX * BY, 1)
       mbar_arrive_expect_tx(&bars[j], box_bytes);
       if (!(hold_cta && j == p.hold_plane))
         tma_load_3d(smem + j * PL, &tmap, tx0, ty0, kb + j, &bars[j]);
+    }
+    if (FR && nit > 1) {  // f of plane kb, first read at iteration 1
+      mbar_arrive_expect_tx(&fbars[0], box_bytes);
+      tma_load_3d(fbase, &p.amap, tx0, ty0, kb, &fbars[0]);
     }
   }
 
@@ -259,7 +286,10 @@ __global__ void __launch_bounds__(BX * BY, 1)
     constexpr int SN = PH, SC = (PH + 2) % 3, SM = (PH + 1) % 3;  // newest, centre, z-1
     const int k = kb + r;
     const int st = r & (NST - 1);
-    const bool to = !mbar_wait_bounded(&bars[st], (r / NST) & 1, p.err, p.wait_ns);
+    bool to = !mbar_wait_bounded(&bars[st], (r / NST) & 1, p.err, p.wait_ns);
+    if (FR && r >= 1 && !to)  // f of plane k - 1, first read by level 1 now
+      to = !mbar_wait_bounded(&fbars[(r - 1) % (FR ? NF : 1)], ((r - 1) / (FR ? NF : 1)) & 1,
+                              p.err, p.wait_ns);
     if (__syncthreads_or(to)) {
       fail_r = r;
       return false;
@@ -269,6 +299,13 @@ __global__ void __launch_bounds__(BX * BY, 1)
       mbar_arrive_expect_tx(&bars[s2], box_bytes);
       if (!(hold_cta && r + LA == p.hold_plane))
         tma_load_3d(smem + s2 * PL, &tmap, tx0, ty0, k + LA, &bars[s2]);
+    }
+    // f of plane k + 1 (read from iteration r + 2 on) into the stage of plane
+    // k + 1 - NF = k - T - 1, whose last reader was level T one iteration ago
+    if (FR && tid == 0 && r + 2 < nit) {
+      const int fs = (r + 1) % (FR ? NF : 1);
+      mbar_arrive_expect_tx(&fbars[fs], box_bytes);
+      tma_load_3d(fbase + fs * PL, &p.amap, tx0, ty0, k + 1, &fbars[fs]);
     }
     // level 0: the input plane k into registers (pair order)
     const float* const sk = smem + st * PL + o_row0;
@@ -306,11 +343,18 @@ __global__ void __launch_bounds__(BX * BY, 1)
         const uint64_t ym1 = e > 0 ? L[SC][e > 0 ? e - 1 : 0][1] : ab1;
         const uint64_t yp0 = e < E - 1 ? L[SC][e < E - 1 ? e + 1 : 0][0] : be0;
         const uint64_t yp1 = e < E - 1 ? L[SC][e < E - 1 ? e + 1 : 0][1] : be1;
-        // x-1, c, x+1, y-1, y+1, z-1, z+1 (opencl/jacobi-3d/jacobi-3d.cpp:282-304)
-        uint64_t s0 = p2_add(xm0, c0);
-        uint64_t s1 = p2_add(c0, c1);
-        s0 = p2_add(s0, c1);
-        s1 = p2_add(s1, xp1);
+        uint64_t s0, s1;
+        if constexpr (FR) {
+          // x-1, x+1, y-1, y+1, z-1, z+1 (OpPoisson3D::star)
+          s0 = p2_add(xm0, c1);
+          s1 = p2_add(c0, xp1);
+        } else {
+          // x-1, c, x+1, y-1, y+1, z-1, z+1 (opencl/jacobi-3d/jacobi-3d.cpp:282-304)
+          s0 = p2_add(xm0, c0);
+          s1 = p2_add(c0, c1);
+          s0 = p2_add(s0, c1);
+          s1 = p2_add(s1, xp1);
+        }
         s0 = p2_add(s0, ym0);
         s1 = p2_add(s1, ym1);
         s0 = p2_add(s0, yp0);
@@ -321,6 +365,22 @@ __global__ void __launch_bounds__(BX * BY, 1)
         s1 = p2_add(s1, L[SN][e][1]);
         O[e][0] = s0;
         O[e][1] = s1;
+      }
+      if constexpr (FR) {  // s + (-h^2) f, f of plane q from its stage
+        const float* const fq = fbase + ((r - t + NF) % (FR ? NF : 1)) * PL + o_row0;
+        const bool fin = (unsigned)q < (unsigned)n2;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          uint64_t f0, f1;
+          p2_lds_nat(fq + e * TX, f0, f1);
+          // the product is masked to the domain before the add: besides
+          // zeroing it outside, the AND between them keeps the compiler from
+          // contracting mul.rn.f32x2 + add.rn.f32x2 into one fused operation
+          // (a single rounding; observed as 1-ulp differences in rare cells)
+          const uint32_t m = fin ? rowmask[e] : 0u;
+          O[e][0] = p2_add(O[e][0], p2_and(p2_mul(nh2, f0), m));
+          O[e][1] = p2_add(O[e][1], p2_and(p2_mul(nh2, f1), m));
+        }
       }
       if (t < T) {
 #pragma unroll
@@ -376,6 +436,12 @@ __global__ void __launch_bounds__(BX * BY, 1)
       // bounded by time only: planes fail_r .. fail_r + LA - 1 were issued
       for (int j = fail_r; j < nit && j < fail_r + LA; ++j)
         mbar_wait_drain(&bars[j & (NST - 1)], (j / NST) & 1, p.wait_ns);
+      // f planes issued but not yet waited for: the failing iteration's
+      // k - 1 and k (issued one iteration before it)
+      if (FR)
+        for (int j = fail_r - 1; j <= fail_r && j < nit - 1; ++j)
+          if (j >= 0)
+            mbar_wait_drain(&fbars[j % (FR ? NF : 1)], (j / (FR ? NF : 1)) & 1, p.wait_ns);
     }
     __syncthreads();
   }

@@ -97,15 +97,20 @@ def pick(grids, cost_model=None, device=0):
     return grids
 
 
-STREAM_MENU = [dict(T=T, by=rows) for T in range(1, 5) for rows in (1, 16, 32, 64, 128)]
+STREAM_MENU = [dict(T=T, by=rows) for T in range(1, 5) for rows in (16, 32, 64, 128)]
+SATURATED_N = 2048  # grid side at which one y-streamed launch fills the B200
 
 
 def pick_stream(grids, cost_model=None, T=4, rows=1, device=0):
     """Stream-mode choice per grid.  With a cost model: the best predicted
     (T, rows per segment) of STREAM_MENU (T 1..4 -- the batch kernel's strip
-    halo covers T <= 4 -- and rows 1 = the library's default, 16 .. 128), from
-    the features of the grid's own y-streamed geometry; without one: T (at
-    most the step count) and `rows`."""
+    halo covers T <= 4 -- and 16 .. 128 rows per segment).  The model is
+    trained on single launches, where a small grid cannot fill the GPU and
+    short segments win by parallelism alone; inside a batch every grid shares
+    a full GPU, so each grid is ranked at its saturated rate: the features of
+    the same (T, rows) geometry on a grid of side max(n, SATURATED_N).
+    Without a model: T (at most the step count) and `rows` (1 = the batch
+    engine's default of 64)."""
     from . import model as M
     for g in grids:
         if cost_model is None:
@@ -117,9 +122,9 @@ def pick_stream(grids, cost_model=None, T=4, rows=1, device=0):
                 continue
             cfg = dict(kernel="stream", T=c["T"], bx=32, by=c["by"], bz=1, E=1)
             try:
-                geo = derive_geometry(stencil=g["stencil"], n=g["n"], steps=g["steps"],
-                                      T=c["T"], bx=32, by=c["by"], bz=1, E=1, kernel="stream",
-                                      device=device)
+                geo = derive_geometry(stencil=g["stencil"], n=max(g["n"], SATURATED_N),
+                                      steps=g["steps"], T=c["T"], bx=32, by=c["by"], bz=1, E=1,
+                                      kernel="stream", device=device)
             except OtsError:
                 continue
             feats.append(M.features(g["stencil"], cfg, geo))

@@ -278,6 +278,33 @@ def test_stream2d_generic_matches_oracle(st, variant, T):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("variant", [0, 2])
+@pytest.mark.parametrize("n,steps,T", [(150, 13, 1), (301, 9, 3), (257, 11, 4), (130, 7, 6)])
+def test_stream2d_rician_two_phase_equals_tile_bitwise(variant, n, steps, T):
+    # the streamed Rician kernel computes g once per cell a row ahead of its
+    # update; the tile kernel (two-phase as well) and the plain kernel (g
+    # recomputed at each neighbour) give the same bits
+    with ots.Plan("rician-denoise-2d", n, steps, T=T, bx=32, by=1, E=1, kernel="stream",
+                  variant=variant) as plan:
+        state, aux = plan.fill_reference(seed=11 + T)
+        g = plan.geometry
+        cut = (slice(g.padding, g.padding + n),) * 2
+        u, f = np.ascontiguousarray(state[0][cut]), np.ascontiguousarray(aux[0][cut])
+        outs = []
+        for k in ("stream", "plain"):
+            plan.upload_interior([u], [f])
+            plan.run(k)
+            outs.append(plan.download_interior()[0])
+    with ots.Plan("rician-denoise-2d", n, steps, T=2, bx=32, by=8, E=2, kernel="tile",
+                  variant=variant) as plan:
+        plan.upload_interior([u], [f])
+        plan.run("tile")
+        outs.append(plan.download_interior()[0])
+    assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
+    assert np.array_equal(outs[0].view(np.uint32), outs[2].view(np.uint32))
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("st", ["jacobi-1d", "jacobi-1d-5pt", "jacobi-1d-7pt"])
 @pytest.mark.parametrize("T,E", [(1, 4), (5, 4), (3, 8), (8, 16), (16, 16)])
 def test_stream1d_register_kernel_matches_oracle(st, T, E):
@@ -459,29 +486,41 @@ def test_full_size_jacobi_3d_tiled_equals_plain_and_fp64_error():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("st", ["jacobi-3d", "poisson-3d"])
 @pytest.mark.parametrize("T", [1, 2, 3, 4])
 @pytest.mark.parametrize("E,bx,by", [(4, 16, 16), (4, 16, 8), (4, 8, 16), (2, 16, 32),
                                      (2, 32, 16), (2, 16, 16)])
-def test_packed_stream_kernel_matches_oracle(T, E, bx, by):
+def test_packed_stream_kernel_matches_oracle(st, T, E, bx, by):
     """The packed-FP32 z-streamed kernel (pairs (v0, v2), (v1, v3) in 64-bit
     registers) in every instantiated block shape: bit for bit against the
     oracle, with n not a multiple of the tile interior, several z segments
-    and a shallower last launch."""
+    and a shallower last launch (Poisson-3D: its f ring as well)."""
+    if st == "poisson-3d":
+        # the f ring (T + 2 planes) beside the state ring and the exchange rows
+        # can exceed a CTA's 227 KB at the tallest tiles: a clean refusal
+        try:
+            ots.derive_geometry(stencil=st, n=132, steps=2 * T + 1, T=T, bx=bx, by=by, bz=1,
+                                E=E, kernel="stream")
+        except ots.OtsError as e:
+            assert e.status_name == "SMEM_TOO_LARGE" and (T, E, bx * by) == (4, 2, 512), (T, E)
+            return
     for n in (60, 132):  # several tiles with partial edge tiles, and z segments
-        g = run_and_check("jacobi-3d", n, 2 * T + 1, T=T, bx=bx, by=by, bz=1, E=E,
-                          kernel="stream")
+        g = run_and_check(st, n, 2 * T + 1, T=T, bx=bx, by=by, bz=1, E=E, kernel="stream")
         assert g.kernel == ots.KERNEL_STREAM
-        with ots.Plan("jacobi-3d", n, 2 * T + 1, T=T, bx=bx, by=by, bz=1, E=E,
+        with ots.Plan(st, n, 2 * T + 1, T=T, bx=bx, by=by, bz=1, E=E,
                       kernel="stream") as plan:
             assert plan.describe()["Stream Arithmetic"] == "packed-fp32"
     # shapes without a packed instantiation, and n % 4 != 0, run the scalar kernel
-    with ots.Plan("jacobi-3d", 60, 5, T=2, bx=32, by=8, bz=1, E=2, kernel="stream") as plan:
+    with ots.Plan(st, 60, 5, T=2, bx=32, by=8, bz=1, E=2, kernel="stream") as plan:
         assert plan.describe()["Stream Arithmetic"] == "scalar"
     try:
-        with ots.Plan("jacobi-3d", 61, 5, T=T, bx=bx, by=by, bz=1, E=E, kernel="stream") as plan:
+        with ots.Plan(st, 61, 5, T=T, bx=bx, by=by, bz=1, E=E, kernel="stream") as plan:
             assert plan.describe()["Stream Arithmetic"] == "scalar"
-    except ots.OtsError as e:  # beyond the scalar kernel's thread limit
-        assert e.status_name == "BLOCK_TOO_LARGE" and bx * by > 256
+    except ots.OtsError as e:
+        # beyond the scalar kernel's thread limit, or (Poisson: its f ring)
+        # beyond a CTA's shared memory
+        assert (e.status_name == "BLOCK_TOO_LARGE" and bx * by > 256) or \
+            (e.status_name == "SMEM_TOO_LARGE" and st == "poisson-3d")
 
 
 @pytest.mark.gpu
@@ -489,24 +528,33 @@ def test_packed_stream_kernel_matches_oracle(T, E, bx, by):
                                                (64, 8, 4, 2, 16, 16), (36, 5, 2, 4, 8, 16),
                                                (200, 4, 3, 2, 16, 32), (4, 6, 4, 4, 16, 16),
                                                (97, 7, 3, 4, 16, 16)])
-def test_packed_and_scalar_stream_kernels_agree_bitwise(n, steps, T, E, bx, by):
+@pytest.mark.parametrize("st", ["jacobi-3d", "poisson-3d"])
+def test_packed_and_scalar_stream_kernels_agree_bitwise(st, n, steps, T, E, bx, by):
     """stream_impl 0 (packed) and 1 (scalar) on the same plan shape: identical
     bits, and both equal to the oracle (the reference weight 0.143 too)."""
     outs = []
     for impl in (0, 1):
-        with ots.Plan("jacobi-3d", n, steps, T=T, bx=bx, by=by, bz=1, E=E, kernel="stream",
-                      impl=impl) as plan:
-            state, _ = plan.fill_reference(seed=21)
-            plan.upload(state)
+        try:
+            plan = ots.Plan(st, n, steps, T=T, bx=bx, by=by, bz=1, E=E, kernel="stream",
+                            impl=impl)
+        except ots.OtsError as e:
+            # the scalar kernel's Poisson f ring needs more shared memory than
+            # the packed kernel's at the tallest tiles
+            assert impl == 1 and st == "poisson-3d" and e.status_name == "SMEM_TOO_LARGE"
+            continue
+        with plan:
+            state, aux = inputs(plan, seed=21)
+            plan.upload(state, aux)
             plan.run()
             outs.append(plan.download()[0])
             g = plan.geometry
-    want = O.sweep_f32("jacobi-3d", state, steps=steps, lo=g.padding, hi=g.padding + g.real_size,
-                       coef=g.coef)[0]
-    assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
-    assert np.array_equal(outs[0].view(np.uint32), want.view(np.uint32))
-    run_and_check("jacobi-3d", 45, 6, T=3, bx=16, by=16, bz=1, E=4, kernel="stream",
-                  variant=ots.VARIANT_REF)
+    want = O.sweep_f32(st, state, aux=aux, steps=steps, lo=g.padding,
+                       hi=g.padding + g.real_size, coef=g.coef, h2=g.h2)[0]
+    for o in outs:
+        assert np.array_equal(o.view(np.uint32), want.view(np.uint32))
+    if st == "jacobi-3d":
+        run_and_check("jacobi-3d", 45, 6, T=3, bx=16, by=16, bz=1, E=4, kernel="stream",
+                      variant=ots.VARIANT_REF)
 
 
 # Fast-division variant (OTS_VARIANT_FAST): __fdividef (2 ulp) and rsqrtf in
