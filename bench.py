@@ -266,7 +266,7 @@ def run_configs(args):
     lines = []
     for w in W.WORKLOADS:
         st = w["stencil"]
-        if want and st not in want:
+        if want and W.workload_key(w) not in want:
             continue
         t_start = time.time()
         done = [0]
@@ -285,7 +285,8 @@ def run_configs(args):
         cm.close()
         plain = W.plain_record(w)
         t_sweep = time.time() - t_start
-        line = {"workload": w["name"], "stencil": st, "n": w["n"], "steps": w["steps"],
+        line = {"workload": w["name"], "stencil": st, "variant": w.get("variant", "baseline"),
+                "n": w["n"], "steps": w["steps"],
                 "space": len(ok), "invalid": len(recs) - len(ok),
                 "exhaustive": {"gupdates": best["gupdates"], "config": W.config_of(best)},
                 "learned": {"gupdates": pk["picked"]["gupdates"],
@@ -390,7 +391,8 @@ def main():
     ap.add_argument("--e2e-depth", type=int, default=3,
                     help="plans in flight in the end-to-end leg (each holds 2 x 537 MB)")
     ap.add_argument("--configs", help="measure the listed workloads (stencil names, comma "
-                    "separated, or 'all') at full size instead of the bench line")
+                    "separated, '<stencil>-fast' for a fast-division row, or 'all') at full "
+                    "size instead of the bench line")
     ap.add_argument("--configs-out", help="write the --configs results to this JSON file")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)

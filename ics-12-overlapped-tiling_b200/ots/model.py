@@ -243,9 +243,14 @@ def plain_values(records):
 
 def workload_records(configs):
     """The full-size workload sweeps of a bench --configs table (its per-
-    workload 'records'), as dataset records with their stencil and size."""
+    workload 'records'), as dataset records with their stencil and size.  Rows
+    in another arithmetic variant (the fast-division ones) are left out: the
+    features do not carry the variant, so their times would contradict the
+    baseline rows'."""
     out = []
     for w in configs.get("workloads", []):
+        if w.get("variant", "baseline") != "baseline":
+            continue
         for r in w.get("records", []):
             out.append(dict(r, stencil=w["stencil"], n=w["n"], steps=w["steps"]))
     return out

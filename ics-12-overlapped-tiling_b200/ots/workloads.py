@@ -16,7 +16,9 @@ Workloads (grid side, time steps):
 
 The last two are held out: each one's picks come from a cost model trained
 without it (the reference's leave-one-out protocol,
-scripts/run-weka.py:74-150).
+scripts/run-weka.py:74-150).  Both, and cs-3d, are measured a second time in
+the fast-division variant (approximate division and rsqrt, within the
+tolerance the parity tests state; key '<stencil>-fast' for --configs).
 The other seven stencils follow at the sizes the training data was measured
 at (1D 4194304 cells x 64, 2D 2048^2 x 64, 3D 256^3 x 32 steps).
 
@@ -35,7 +37,7 @@ import os
 
 import numpy as np
 
-from . import OtsError, Plan
+from . import VARIANT_FAST, OtsError, Plan
 from . import model as M
 from .dataset import space
 from .sweep import make_inputs
@@ -60,7 +62,25 @@ WORKLOADS = [
     dict(name="gradient-2d 2048^2 x 64", stencil="gradient-2d", n=2048, steps=64, extra=True),
     dict(name="gradient-3d 256^3 x 32", stencil="gradient-3d", n=256, steps=32, extra=True),
     dict(name="cs-3d 256^3 x 32", stencil="cs-3d", n=256, steps=32, extra=True),
+    # the fast-division variant of the three stencils that divide
+    dict(name="rician-denoise-2d 4096^2 x 200 (fast division)", stencil="rician-denoise-2d",
+         n=4096, steps=200, held_out=True, variant="fast"),
+    dict(name="cdsc-tv-update-2d 4096^2 x 200 (fast division)", stencil="cdsc-tv-update-2d",
+         n=4096, steps=200, held_out=True, variant="fast"),
+    dict(name="cs-3d 256^3 x 32 (fast division)", stencil="cs-3d", n=256, steps=32,
+         extra=True, variant="fast"),
 ]
+
+
+def workload_key(w):
+    """The --configs selector of a workload: its stencil, '-fast' appended
+    for the fast-division rows."""
+    return w["stencil"] + ("-fast" if w.get("variant") == "fast" else "")
+
+
+def variant_kw(w):
+    """Plan keywords of the workload's arithmetic variant (none: baseline)."""
+    return {"variant": VARIANT_FAST} if w.get("variant") == "fast" else {}
 HELD_OUT = ("rician-denoise-2d", "cdsc-tv-update-2d")
 
 # compulsory bytes per update of a one-step launch: read every field once,
@@ -127,7 +147,7 @@ def sweep_workload(w, cfgs=None, device=0, log=None):
     for cfg in cfgs or space(st, dims):
         rec = dict(stencil=st, n=n, steps=steps, **cfg)
         try:
-            plan = Plan(st, n, steps, device=device, **cfg)
+            plan = Plan(st, n, steps, device=device, **variant_kw(w), **cfg)
         except OtsError as e:
             rec.update(status=e.status_name)
             recs.append(rec)
@@ -206,7 +226,7 @@ def learned_pick(w, cost_model, k_frac=0.10, device=0):
             plain = cfg
             continue
         try:
-            g = derive_geometry_for(st, n, steps, cfg, device)
+            g = derive_geometry_for(st, n, steps, cfg, device, **variant_kw(w))
         except OtsError:
             continue
         cands.append(cfg)
@@ -220,11 +240,11 @@ def learned_pick(w, cost_model, k_frac=0.10, device=0):
     return max(ok, key=lambda r: r["gupdates"]), k, size
 
 
-def derive_geometry_for(stencil, n, steps, cfg, device=0):
+def derive_geometry_for(stencil, n, steps, cfg, device=0, **kw):
     from . import derive_geometry
     return derive_geometry(stencil=stencil, n=n, steps=steps, T=cfg["T"], bx=cfg["bx"],
                            by=cfg["by"], bz=cfg["bz"], E=cfg["E"], kernel=cfg["kernel"],
-                           device=device)
+                           device=device, **kw)
 
 
 def config_of(rec):
@@ -242,7 +262,7 @@ def run_config(w, cfg, device=0):
     """(plan geometry, padded inputs, padded outputs) of one full run of the
     workload with `cfg`; the inputs come back padded so a CPU sweep can
     start from the same state."""
-    with Plan(w["stencil"], w["n"], w["steps"], device=device, **cfg) as plan:
+    with Plan(w["stencil"], w["n"], w["steps"], device=device, **variant_kw(w), **cfg) as plan:
         g = plan.geometry
         st, ax = inputs(plan)
         plan.upload_interior(st, ax)

@@ -101,8 +101,8 @@ typedef enum ots_kernel {
  * source.  OTS_VARIANT_REF: the reference kernels' arithmetic (0.143f; 8c-sum8 and
  * 26c-sum26; +Ey in the Hz update, no source).  OTS_VARIANT_FAST (rician-denoise-2d,
  * cdsc-tv-update-2d, cs-3d only): the baseline arithmetic with every division
- * replaced by CUDA's approximate division (__fdividef, 2 ulp) and cs-3d's 1/sqrt
- * terms in float rsqrt -- the latitude the reference's OpenCL build gave its
+ * replaced by the approximate PTX division (div.approx.ftz.f32, 2 ulp;
+ * subnormals flushed) and cs-3d's 1/sqrt terms in float rsqrt -- the latitude the reference's OpenCL build gave its
  * kernels (default options, single-precision '/' within 2.5 ulp;
  * opencl/rician-denoise-2d/rician-denoise-2d.cpp:662); results are no longer
  * bit-reproducible against an IEEE CPU loop, only within the tolerance the

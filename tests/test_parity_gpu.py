@@ -557,8 +557,8 @@ def test_packed_and_scalar_stream_kernels_agree_bitwise(st, n, steps, T, E, bx, 
                       variant=ots.VARIANT_REF)
 
 
-# Fast-division variant (OTS_VARIANT_FAST): __fdividef (2 ulp) and rsqrtf in
-# place of IEEE division / correctly rounded 1/sqrt.  Bound on
+# Fast-division variant (OTS_VARIANT_FAST): div.approx.ftz.f32 (2 ulp) and
+# the approximate rsqrt in place of IEEE division / correctly rounded 1/sqrt.  Bound on
 # max |gpu - cpu| / max(|cpu|, 1) against the IEEE FP32 oracle after the step
 # counts used here (relative above 1, absolute below; these stencils' values
 # lie in [0, 1) on the reference fill, so the bound is absolute).

@@ -71,9 +71,17 @@ def test_picks_keep_best_measured_of_top_k():
 
 
 def test_workload_table_names_every_configured_stencil():
-    names = [w["stencil"] for w in W.WORKLOADS if not w.get("extra")]
+    base = [w for w in W.WORKLOADS if "variant" not in w]
+    names = [w["stencil"] for w in base if not w.get("extra")]
     assert names == ["jacobi-2d", "jacobi-3d", "poisson-3d", "fdtd-2d", "rician-denoise-2d",
                      "cdsc-tv-update-2d"]
-    assert sorted(w["stencil"] for w in W.WORKLOADS) == sorted(ots.STENCILS)
+    assert sorted(w["stencil"] for w in base) == sorted(ots.STENCILS)
+    # the fast-division rows: the three stencils that divide, each key unique
+    fast = [w for w in W.WORKLOADS if w.get("variant") == "fast"]
+    assert sorted(w["stencil"] for w in fast) == ["cdsc-tv-update-2d", "cs-3d",
+                                                  "rician-denoise-2d"]
+    keys = [W.workload_key(w) for w in W.WORKLOADS]
+    assert len(set(keys)) == len(keys) and "rician-denoise-2d-fast" in keys
+    assert W.variant_kw(fast[0]) == {"variant": ots.VARIANT_FAST} and W.variant_kw(base[0]) == {}
     assert all(w["stencil"] in W.BYTES_PER_UPDATE for w in W.WORKLOADS)
     assert set(W.HELD_OUT) == {w["stencil"] for w in W.WORKLOADS if w.get("held_out")}
