@@ -17,9 +17,10 @@
 //     is then a whole pair: the centre, the rows above and below and the
 //     planes below and above (same x), and the x neighbour inside the thread
 //     ((v1, v3) is the right neighbour of (v0, v2), which is the left
-//     neighbour of (v1, v3)).  Only (v0, v2)'s left neighbour (v-1, v1) and
-//     (v1, v3)'s right neighbour (v2, v4) are assembled, each from one
-//     shuffled and one own value;
+//     neighbour of (v1, v3)).  The two adds that take (v0, v2)'s left
+//     neighbours (v-1, v1) or (v1, v3)'s right neighbours (v2, v4) run as
+//     scalar adds writing the halves of a pair, so no neighbour pair has to
+//     be assembled;
 //   * the rows other threads read (a thread's first and last row) go through
 //     a compact exchange buffer in this pair order, so they load straight into
 //     pairs (ld.shared.v2.b64);
@@ -139,7 +140,8 @@ inline int shape3p_index(int E, int BX, int BY) {
 //   thread row's first and last, pair order), TX floats each,
 //   ops with an aux field: T + 2 f stages (TX x TY floats each),
 //   NST mbarriers, then one per f stage.
-// NST is 8 where that fits the 227 KB a CTA may use, else 4.
+// NST is 8 where that fits the 227 KB a CTA may use, else 4 (and 4 where
+// that lets two small CTAs share an SM, below).
 constexpr size_t kSmemPerCta = 227 * 1024;
 __host__ __device__ constexpr size_t stream3p_stage_floats(int TX, int TY) {
   return (size_t)(TX * TY + 31) / 32 * 32;
@@ -154,8 +156,22 @@ __host__ __device__ constexpr size_t stream3p_bytes(int nst, int T, int TX, int 
           stream3p_xbuf_floats(T, TX, BY)) * 4 +
          (size_t)(nst + stream3p_aux_stages(T, na)) * 8;
 }
+// Blocks of at most 128 threads can run two to an SM (their registers fit
+// twice even at 255 a thread): they take the deeper ring only where two CTAs
+// still fit the SM's 228 KB (each with the launch's 128 bytes of alignment
+// slack and the 1 KB the SM reserves per CTA).  The ring depth barely matters
+// (8 stages against 4: within 1 %), occupancy does (Poisson-3D at 16 x 8,
+// E = 4, T = 4: one CTA per SM with 8 stages, two with 4).
+constexpr size_t kSmemPerSm = 228 * 1024;
+__host__ __device__ constexpr bool stream3p_two_fit(size_t bytes) {
+  return 2 * (bytes + 128 + 1024) <= kSmemPerSm;
+}
 __host__ __device__ constexpr int stream3p_stages(int T, int TX, int TY, int BY, int na) {
-  return stream3p_bytes(8, T, TX, TY, BY, na) <= kSmemPerCta ? 8 : 4;
+  return ((TX / 4) * BY <= 128 && !stream3p_two_fit(stream3p_bytes(8, T, TX, TY, BY, na)) &&
+          stream3p_two_fit(stream3p_bytes(4, T, TX, TY, BY, na)))
+             ? 4
+         : stream3p_bytes(8, T, TX, TY, BY, na) <= kSmemPerCta ? 8
+                                                              : 4;
 }
 __host__ __device__ constexpr size_t stream3p_smem_bytes(int T, int TX, int TY, int BY,
                                                          int na) {
@@ -335,25 +351,27 @@ __global__ void __launch_bounds__(BX * BY, 1)
       for (int e = 0; e < E; ++e) {
         const uint64_t c0 = L[SC][e][0], c1 = L[SC][e][1];  // (v0, v2), (v1, v3)
         // x neighbours: (v-1, v1) and (v2, v4); v-1 / v4 from the lanes beside
-        const float left = __shfl_up_sync(0xffffffffu, p2_hi(c1), 1);
-        const float right = __shfl_down_sync(0xffffffffu, p2_lo(c0), 1);
-        const uint64_t xm0 = p2_make(left, p2_lo(c1));
-        const uint64_t xp1 = p2_make(p2_hi(c0), right);
+        const float v0 = p2_lo(c0), v2 = p2_hi(c0), v1 = p2_lo(c1), v3 = p2_hi(c1);
+        // x neighbours v-1 / v4 from the lanes beside
+        const float left = __shfl_up_sync(0xffffffffu, v3, 1);
+        const float right = __shfl_down_sync(0xffffffffu, v0, 1);
         const uint64_t ym0 = e > 0 ? L[SC][e > 0 ? e - 1 : 0][0] : ab0;
         const uint64_t ym1 = e > 0 ? L[SC][e > 0 ? e - 1 : 0][1] : ab1;
         const uint64_t yp0 = e < E - 1 ? L[SC][e < E - 1 ? e + 1 : 0][0] : be0;
         const uint64_t yp1 = e < E - 1 ? L[SC][e < E - 1 ? e + 1 : 0][1] : be1;
+        // The adds that involve a shuffled neighbour are scalar, written
+        // straight into the halves of a new pair; assembling the neighbour
+        // pairs (v-1, v1) and (v2, v4) instead would cost register moves.
         uint64_t s0, s1;
         if constexpr (FR) {
           // x-1, x+1, y-1, y+1, z-1, z+1 (OpPoisson3D::star)
-          s0 = p2_add(xm0, c1);
-          s1 = p2_add(c0, xp1);
+          s0 = p2_make(left + v1, v1 + v3);
+          s1 = p2_make(v0 + v2, v2 + right);
         } else {
           // x-1, c, x+1, y-1, y+1, z-1, z+1 (opencl/jacobi-3d/jacobi-3d.cpp:282-304)
-          s0 = p2_add(xm0, c0);
-          s1 = p2_add(c0, c1);
-          s0 = p2_add(s0, c1);
-          s1 = p2_add(s1, xp1);
+          s0 = p2_add(p2_make(left + v0, v1 + v2), c1);
+          const uint64_t t = p2_add(c0, c1);
+          s1 = p2_make(p2_lo(t) + v2, p2_hi(t) + right);
         }
         s0 = p2_add(s0, ym0);
         s1 = p2_add(s1, ym1);

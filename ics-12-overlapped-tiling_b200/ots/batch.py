@@ -97,20 +97,26 @@ def pick(grids, cost_model=None, device=0):
     return grids
 
 
-STREAM_MENU = [dict(T=T, by=rows) for T in range(1, 5) for rows in (16, 32, 64, 128)]
-SATURATED_N = 2048  # grid side at which one y-streamed launch fills the B200
+# Rows per segment are the batch's own choice, not a grid's: a lone grid
+# wants short segments for parallelism (16 rows is the single-launch optimum
+# at 2048^2), but in a batch hundreds of grids share the GPU, and short
+# segments only add halo rows (2 R T per segment: +50 % at 16 rows, T = 4;
+# measured on the 256-grid batch at T = 4: 16 rows 673, 32 rows 805, 64 rows
+# 918, 128 rows 908, 256 rows 807 GUpd/s).  The batch engine's 64 stays.
+STREAM_ROWS = 64
+STREAM_MENU = [dict(T=T, by=STREAM_ROWS) for T in range(1, 5)]
+SATURATED_N = 2048  # grid side at which the model ranks (inside a batch the GPU is full)
 
 
 def pick_stream(grids, cost_model=None, T=4, rows=1, device=0):
-    """Stream-mode choice per grid.  With a cost model: the best predicted
-    (T, rows per segment) of STREAM_MENU (T 1..4 -- the batch kernel's strip
-    halo covers T <= 4 -- and 16 .. 128 rows per segment).  The model is
-    trained on single launches, where a small grid cannot fill the GPU and
-    short segments win by parallelism alone; inside a batch every grid shares
-    a full GPU, so each grid is ranked at its saturated rate: the features of
-    the same (T, rows) geometry on a grid of side max(n, SATURATED_N).
-    Without a model: T (at most the step count) and `rows` (1 = the batch
-    engine's default of 64)."""
+    """Stream-mode choice per grid.  With a cost model: the T (1..4 -- the
+    batch kernel's strip halo covers T <= 4) the model predicts fastest for
+    the grid's stencil at STREAM_ROWS rows per segment.  The model is trained
+    on single launches, where a small grid cannot fill the GPU; inside a
+    batch every grid shares a full GPU, so each grid is ranked at its
+    saturated rate: the features of the same geometry on a grid of side
+    max(n, SATURATED_N).  Without a model: T (at most the step count) and
+    `rows` (1 = the batch engine's default of 64)."""
     from . import model as M
     for g in grids:
         if cost_model is None:
