@@ -93,29 +93,48 @@ def profile_traffic(kernel):
 
 
 class Clocks:
-    """Samples nvidia-smi during the timed region."""
+    """Samples nvidia-smi (with its timestamps) around the timed region.
+    nvidia-smi takes a moment to start, so the sampler is started first and
+    the timed region begins only once the first sample is in; mark() brackets
+    the region, and the summary keeps the samples taken inside it (at least
+    the one before and the one after)."""
+
+    FIELDS = ("timestamp,clocks.sm,clocks.max.sm,power.draw,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index):
         self.index = index
         self.proc = None
         self.path = os.path.join("/tmp", "ots_clocks_%d.csv" % os.getpid())
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index),
-                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
-                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=self.fh, stderr=subprocess.DEVNULL)
+            deadline = time.time() + 10.0
+            while time.time() < deadline and self.proc.poll() is None:
+                self.fh.flush()
+                if os.path.getsize(self.path) > 0:
+                    break
+                time.sleep(0.05)
         except Exception:
             self.proc = None
         return self
 
+    def mark(self, which):
+        if which == "start":
+            self.t0 = time.time()
+        else:
+            self.t1 = time.time()
+
     def __exit__(self, *a):
         if self.proc is not None:
+            time.sleep(0.1)  # one more sample after the region
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -126,23 +145,39 @@ class Clocks:
         except Exception:
             pass
 
+    @staticmethod
+    def _stamp(text):
+        import datetime
+        try:
+            return datetime.datetime.strptime(text, "%Y/%m/%d %H:%M:%S.%f").timestamp()
+        except ValueError:
+            return None
+
     def summary(self):
         rows = []
         try:
             for line in open(self.path):
                 parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 7:
-                    rows.append(parts)
+                if len(parts) >= 8:
+                    rows.append((self._stamp(parts[0]), parts[1:]))
         except Exception:
             pass
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        sm = sorted(float(r[0]) for r in rows if r[0].replace(".", "").isdigit())
-        mx = max(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
+        inside = rows
+        if self.t0 is not None and self.t1 is not None and all(t is not None for t, _ in rows):
+            inside = [r for r in rows if self.t0 <= r[0] <= self.t1]
+            before = [r for r in rows if r[0] < self.t0][-1:]
+            after = [r for r in rows if r[0] > self.t1][:1]
+            if not inside:
+                inside = before + after
+        vals = [v for _, v in inside]
+        sm = sorted(float(r[0]) for r in vals if r[0].replace(".", "").isdigit())
+        mx = max((float(r[1]) for r in vals if r[1].replace(".", "").isdigit()), default=None)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[3 + i] == "Active"})
+        reasons = sorted({names[i] for r in vals for i in range(4) if r[3 + i] == "Active"})
         return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(vals)}
 
 
 def dist_setup():
@@ -382,7 +417,7 @@ def run_configs(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
@@ -440,7 +475,9 @@ def main():
         plan.run_async(cfg["kernel"])
     plan.sync()
     with Clocks(local) as clk:
+        clk.mark("start")
         el = timed(cfg["kernel"], args.steps)
+        clk.mark("end")
     el_max = reduce_max(el, world)
     value = job_value(float(N) ** 3 * STEPS * args.steps, world, el_max)
     avg_launch = el / (args.steps * launches_per_step)

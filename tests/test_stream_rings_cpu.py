@@ -9,6 +9,10 @@ stage g - 1.  Aux ring (Poisson's f): NF = T + 2 slots; f of plane k + 1 is
 issued at iteration r, f of plane k - 1 is waited for at the top of r, and
 level t reads f of plane k - t.
 
+The packed kernel (stream3p_kernel in csrc/ots_stream3p.cuh) uses the same
+two rings with NST = 8 or 4 state stages (copies LA = NST - 2 planes ahead)
+and one segment per CTA; it is replayed with those depths below.
+
 Asserted: every read the output depends on finds its plane, already waited
 for, in its slot; no copy is issued into a slot that is read in the same
 iteration (the copy is asynchronous and may land at once); a copy is only
@@ -21,7 +25,7 @@ import pytest
 NST, LA = 4, 2
 
 
-def run_segments(T, nits):
+def run_segments(T, nits, NST=NST, LA=LA):
     NF = T + 2
     slot = [None] * NF            # plane index (running g) whose copy was issued into the slot
     waited = [True] * NF          # the slot's last issued copy has been waited for
@@ -84,6 +88,14 @@ def test_stream_rings_never_overwrite_a_live_plane(T):
         nit = z + 2 * T  # planes of a segment: its z range plus T of fill each side
         run_segments(T, [nit])
         run_segments(T, [nit, nit, nit - 1 if nit > 2 else nit])
+
+
+@pytest.mark.parametrize("T", range(1, 5))
+@pytest.mark.parametrize("nst", [4, 8])
+def test_packed_kernel_rings_never_overwrite_a_live_plane(T, nst):
+    # one segment per CTA (the packed kernel's grid covers the z segments)
+    for z in (1, 2, 3, 5, 8, 17, 40, 64, 128, 512):
+        run_segments(T, [z + 2 * T], NST=nst, LA=nst - 2)
 
 
 def drain_planes(rg, nit, fail_r, NF):
