@@ -105,7 +105,7 @@ def geometry():
 
 # Generated-kernel cases: (stencil, n, T, bx, by, bz, E, steps, seed, oracle variant).
 # Constraints that keep each case clear of the reference kernels' known
-# defects (SURVEY Appendix A is not needed to read them; each is stated):
+# defects (each stated with the kernel lines it concerns):
 #   * 3D: bx == bz, so the local array declared [sZ][sY][sZ] has the shape
 #     the kernel indexes ([sZ][sY][sX], opencl/jacobi-3d/jacobi-3d.cpp:189-190);
 #   * 3D at T = 2: one tile along z (n == bz - 2), so the write-back that
