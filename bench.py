@@ -80,6 +80,26 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def bound_at_T(stencil, T, bytes_per_update, hbm_gbs, sm_count=148):
+    """The roofline that bounds a configuration at time-tile depth T:
+    min(HBM x T / B_u, FP32 / F_u) in GUpdates/s -- a launch reads and writes
+    B_u bytes per cell once and advances T steps; FP32 = SMs x 128 lanes x
+    the maximum SM clock (MEASURED_PEAKS.json sm_max_mhz), one scalar
+    operation per lane and clock; F_u the operations per update of the
+    measured (baseline) arithmetic."""
+    sys.path.insert(0, os.path.join(ROOT, "ics-12-overlapped-tiling_b200"))
+    from ots.model import STENCIL_COST
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            mhz = float(json.load(fh).get("sm_max_mhz", 1965.0))
+    except Exception:
+        mhz = 1965.0
+    mem = hbm_gbs * T / bytes_per_update
+    fp = sm_count * 128 * mhz * 1e6 / STENCIL_COST[stencil][0] / 1e9
+    return {"gupdates": min(mem, fp), "bound": "hbm" if mem <= fp else "fp32",
+            "hbm_x_T_over_bytes": mem, "fp32_over_ops": fp, "T": T}
+
+
 def profile_traffic(kernel):
     """DRAM bytes per launch from the committed ncu summary, if present."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
@@ -340,6 +360,9 @@ def run_configs(args):
         line["one_step_hbm_roofline"] = {
             "gupdates": peak / bpu, "bytes_per_update": bpu, "peak_gbs": peak,
             "peak_source": peak_src, "best_over_roofline": best["gupdates"] / (peak / bpu)}
+        bt = bound_at_T(st, best["T"], bpu, peak)
+        bt["best_over_bound"] = best["gupdates"] / bt["gupdates"]
+        line["bound_T"] = bt
         if st == "jacobi-2d":  # the T sweep at 16 x 16 blocks the workload names
             ts = W.sweep_workload(w, [dict(kernel="tile", T=T, bx=16, by=16, bz=1, E=1)
                                       for T in range(1, 9)])

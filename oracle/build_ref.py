@@ -1,8 +1,9 @@
 #!/usr/bin/env python3
 """Build recipe for oracle/_ref: the reference's own CPU verification loops.
 
-TEST INFRASTRUCTURE ONLY.  Run in a container where the reference checkout
-is present (default /root/reference, or $OTS_REFERENCE_DIR).  For each pinned
+TEST INFRASTRUCTURE ONLY.  Run where a reference checkout is present; its
+location comes from the caller (build(ref_root)) or $OTS_REFERENCE_DIR, and
+without either nothing is built.  For each pinned
 stencil it copies the CPU loop of the reference runner -- the lines between
 ``memcpy(refB, hostData, arraySize);`` and ``memcpy(reference, refA,
 arraySize);`` of its main() -- verbatim into ``oracle/_ref/<name>_loop.inc``
@@ -250,8 +251,8 @@ def build_cuda_jacobi2d(ref_root, nvcc="nvcc"):
 
 
 def build(ref_root=None, cxx="g++", verbose=False):
-    ref_root = ref_root or os.environ.get("OTS_REFERENCE_DIR", "/root/reference")
-    if not os.path.isdir(os.path.join(ref_root, "opencl")):
+    ref_root = ref_root or os.environ.get("OTS_REFERENCE_DIR")
+    if not ref_root or not os.path.isdir(os.path.join(ref_root, "opencl")):
         if verbose:
             print("build_ref: reference tree not present; keeping prebuilt oracle/_ref")
         return False

@@ -166,7 +166,8 @@ def kernels():
 
 if __name__ == "__main__":
     if not build_ref.build(verbose=True):
-        sys.exit("reference tree not found; golden fixtures are generated where it exists")
+        sys.exit("reference tree not found: set OTS_REFERENCE_DIR to the reference checkout "
+                 "(the golden fixtures are generated where it exists)")
     which = sys.argv[1:] or ["loops", "fills", "geometry", "kernels"]
     for name in which:
         {"loops": loops, "fills": fills, "geometry": geometry, "kernels": kernels}[name]()
