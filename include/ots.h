@@ -135,9 +135,11 @@ typedef struct ots_params {
                                   * E rows, so the 2T-row y halo is recomputed
                                   once per cluster instead of once per CTA. */
   int32_t stream_impl;         /* 3D stream kernel implementation: 0 = the
-                                  packed-FP32 kernel where it applies (jacobi-3d,
-                                  E 2 or 4, T <= 4, no clusters, at most 256
-                                  threads), else the scalar one; 1 = always the
+                                  packed-FP32 kernel where it applies (jacobi-3d
+                                  and poisson-3d, T <= 4, no clusters, n a
+                                  multiple of 4, the block shapes 16x16, 16x8,
+                                  8x16 at E = 4 and 16x32, 32x16, 16x16 at
+                                  E = 2), else the scalar one; 1 = always the
                                   scalar kernel.  Both give identical bits. */
   int32_t reserved[5];         /* must be zero */
 } ots_params;
