@@ -350,7 +350,6 @@ __global__ void __launch_bounds__(BX * BY, 1)
 #pragma unroll
       for (int e = 0; e < E; ++e) {
         const uint64_t c0 = L[SC][e][0], c1 = L[SC][e][1];  // (v0, v2), (v1, v3)
-        // x neighbours: (v-1, v1) and (v2, v4); v-1 / v4 from the lanes beside
         const float v0 = p2_lo(c0), v2 = p2_hi(c0), v1 = p2_lo(c1), v3 = p2_hi(c1);
         // x neighbours v-1 / v4 from the lanes beside
         const float left = __shfl_up_sync(0xffffffffu, v3, 1);
