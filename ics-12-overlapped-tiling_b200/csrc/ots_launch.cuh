@@ -66,6 +66,10 @@ struct StencilKernels {
   AttrFn stream3p_attr[kMaxT3p + 1][kShapes3p] = {};
   Occ3pFn stream3p_occ[kMaxT3p + 1][kShapes3p] = {};
   Stream2dLaunch stream2d[kMaxT + 1] = {};  // [T], 2D star stencils
+  // packed-FP32 form of the 2D star kernel (Jacobi-2D, Poisson-2D; n0 % 4 == 0)
+  Stream2dLaunch stream2dp[kMaxT + 1] = {};
+  AttrFn stream2dp_attr[kMaxT + 1] = {};
+  Occ2dFn stream2dp_occ[kMaxT + 1] = {};
   AttrFn stream2d_attr[kMaxT + 1] = {};
   Occ2dFn stream2d_occ[kMaxT + 1] = {};
   Stream2dgLaunch stream2dg[kMaxTg + 1] = {};  // [T], any 2D stencil through apply()
@@ -261,6 +265,22 @@ cudaError_t occ_stream2d(int* blocks) {
                                                        kStream2dThreads, 0);
 }
 
+template <class Op, int T>
+cudaError_t launch_stream2dp(const Stream2dParams& p, dim3 g, cudaStream_t s) {
+  return launch_k(stream2dp_kernel<Op, T>, g, dim3(kStream2dThreads), 0, s, 1, p);
+}
+
+template <class Op, int T>
+cudaError_t attr_stream2dp(cudaFuncAttributes* a) {
+  return cudaFuncGetAttributes(a, stream2dp_kernel<Op, T>);
+}
+
+template <class Op, int T>
+cudaError_t occ_stream2dp(int* blocks) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, stream2dp_kernel<Op, T>,
+                                                       kStream2dThreads, 0);
+}
+
 template <class Op, int V>
 cudaError_t launch_stream1d(const Stream1dParams& p, dim3 g, cudaStream_t s) {
   return launch_k(stream1d_kernel<Op, V>, g, dim3(kStream1dThreads), 0, s, 1, p);
@@ -312,6 +332,14 @@ void fill_stream2dg(StencilKernels& k, std::integer_sequence<int, Ts...>) {
 }
 
 template <class Op, int... Ts>
+void fill_stream2dp(StencilKernels& k, std::integer_sequence<int, Ts...>) {
+  ((k.stream2dp[Ts + 1] = &launch_stream2dp<Op, Ts + 1>,
+    k.stream2dp_attr[Ts + 1] = &attr_stream2dp<Op, Ts + 1>,
+    k.stream2dp_occ[Ts + 1] = &occ_stream2dp<Op, Ts + 1>),
+   ...);
+}
+
+template <class Op, int... Ts>
 void fill_stream2d(StencilKernels& k, std::integer_sequence<int, Ts...>) {
   ((k.stream2d[Ts + 1] = &launch_stream2d<Op, Ts + 1>,
     k.stream2d_attr[Ts + 1] = &attr_stream2d<Op, Ts + 1>,
@@ -349,6 +377,8 @@ StencilKernels make_kernels() {
     fill_tex<Op>(k, std::make_integer_sequence<int, kTexMaxE>{});
   if constexpr (Op::DIMS == 2 && HasStar2D<Op>::value)
     fill_stream2d<Op>(k, std::make_integer_sequence<int, kMaxT>{});
+  if constexpr (Op::DIMS == 2 && Packed2D<Op>::value)
+    fill_stream2dp<Op>(k, std::make_integer_sequence<int, kMaxT>{});
   // the generic streamed kernel where the five-point form does not cover the
   // op (several fields, aux fields, or other neighbours)
   if constexpr (Op::DIMS == 2 && (Op::NS > 1 || Op::NA > 0 || !HasStar2D<Op>::value))

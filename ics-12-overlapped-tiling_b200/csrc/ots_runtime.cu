@@ -177,6 +177,7 @@ struct Stream2dCfg {
   int T = 0, hx = 0, rpbx = 0, ntx = 0, nseg = 0, zseg = 0, grid = 0;
   int warps_per_sm = 0;
   bool generic = false;  // stream2dg_kernel (the op's apply through register rows)
+  bool packed = false;   // stream2dp_kernel (packed FP32 five-point form)
   int R = 1;             // rows of reach per level
 };
 
@@ -401,11 +402,17 @@ ots_status derive_stream2d(const ots_plan* pl, int T, Stream2dCfg* c) {
   c->rpbx = ots::kStream2dWidth - 2 * c->hx;
   const int n = pl->geo.real_size;
   c->ntx = ceil_div(n, c->rpbx);
+  // the packed form needs n0 % 4 == 0 (a lane's four cells all inside or all
+  // outside); stream_impl 1 keeps the scalar kernel
+  c->packed = !c->generic && pl->prm.stream_impl != 1 && n % 4 == 0 &&
+              pl->K->stream2dp[T] != nullptr;
   int blocks = 0;
   const bool fast = pl->prm.variant == OTS_VARIANT_FAST;
   cudaError_t oe = cudaErrorInvalidValue;
   if (c->generic && pl->K->stream2dg_occ[T])
     oe = pl->K->stream2dg_occ[T](&blocks, fast);
+  else if (c->packed && pl->K->stream2dp_occ[T])
+    oe = pl->K->stream2dp_occ[T](&blocks);
   else if (!c->generic && pl->K->stream2d_occ[T])
     oe = pl->K->stream2d_occ[T](&blocks);
   if (oe != cudaSuccess || blocks < 1) blocks = 1;
@@ -675,7 +682,7 @@ void fill_geometry_for_kernel(ots_plan* pl) {
       if (attr && attr(&a, pl->prm.variant == OTS_VARIANT_FAST) == cudaSuccess)
         g.registers = a.numRegs;
     } else {
-      auto attr = pl->K->stream2d_attr[c.T];
+      auto attr = c.packed ? pl->K->stream2dp_attr[c.T] : pl->K->stream2d_attr[c.T];
       if (attr && attr(&a) == cudaSuccess) g.registers = a.numRegs;
     }
     g.ctas_per_sm = c.warps_per_sm / (ots::kStream2dThreads / 32);
@@ -837,7 +844,8 @@ ots_status enqueue_run(ots_plan* pl, int kernel) {
         sp.zseg = c.zseg;
         sp.base_step = base;
         sp.op = pl->op;
-        e = pl->K->stream2d[Tl](sp, dim3(c.grid), pl->stream);
+        e = (c.packed ? pl->K->stream2dp[Tl] : pl->K->stream2d[Tl])(sp, dim3(c.grid),
+                                                                     pl->stream);
       }
       pl->cur ^= 1;
     }
@@ -1587,8 +1595,9 @@ ots_status ots_describe(const ots_plan* plan, ots_kv_fn kv, void* user) {
   emit_i("Register Usage", g.registers);
   static const char* kKernel[] = {"auto", "tile", "stream", "plain", "tex"};
   kv("Kernel", kKernel[(g.kernel >= 0 && g.kernel <= 4) ? g.kernel : 0], user);
-  if (g.kernel == OTS_KERNEL_STREAM && g.dims == 3)
-    kv("Stream Arithmetic", plan->scfg.packed ? "packed-fp32" : "scalar", user);
+  if (g.kernel == OTS_KERNEL_STREAM && (g.dims == 3 || g.dims == 2))
+    kv("Stream Arithmetic",
+       (g.dims == 3 ? plan->scfg.packed : plan->s2cfg.packed) ? "packed-fp32" : "scalar", user);
   emit_i("Dynamic Shared Bytes", g.shared_bytes);
   kv("Engine", p.engine == OTS_ENGINE_COMPAT ? "compat" : "native", user);
   kv("Variant", p.variant == OTS_VARIANT_REF ? "ref"

@@ -21,6 +21,7 @@
 
 #include <type_traits>
 
+#include "ots_pair.cuh"
 #include "ots_tile.cuh"
 
 namespace ots {
@@ -218,6 +219,139 @@ __global__ void __launch_bounds__(kStream2dThreads)
   const int w = blockIdx.x * (kStream2dThreads / 32) + (threadIdx.x >> 5);
   if (w >= p.ntx * p.nseg) return;  // whole warps only
   stream2d_body<Op, T, kLoadLdg>(p, w % p.ntx, w / p.ntx);
+}
+
+// ------------------------------------------------------------------------
+// The same y-streamed scheme with packed FP32 arithmetic, for the two
+// five-point stencils whose update is adds and multiplies only (Jacobi-2D;
+// Poisson-2D with its right-hand side).  A lane's four cells v0..v3 are held
+// as the pairs (v0, v2) and (v1, v3) in 64-bit registers, as in the packed 3D
+// kernel (ots_stream3p.cuh): each add.rn.f32x2 / mul.rn.f32x2 does two IEEE
+// operations, bit for bit the scalar ones, in the op's operand order; the
+// adds that take a shuffled x neighbour (v-1 or v4) run scalar into the halves
+// of a new pair.  Requires n0 % 4 == 0 (the host runs the scalar kernel
+// otherwise), so a lane's four cells are all inside the domain or all
+// outside: the zero ring is one 32-bit AND per pair half and level, all ones
+// or zero -- and that AND between a level's multiply and the next level's
+// adds also keeps the two from being fused into one rounding.  Level T's
+// multiply is scalar, so its results land in natural x order for one 16-byte
+// store.
+template <class Op>
+struct Packed2D
+    : std::bool_constant<std::is_same_v<Op, OpJacobi2D> || std::is_same_v<Op, OpPoisson2D>> {};
+
+template <class Op, int T, int LD>
+__device__ __forceinline__ void stream2dp_body(const Stream2dParams& p, int strip, int seg) {
+  static_assert(Packed2D<Op>::value, "packed form written for Jacobi-2D and Poisson-2D");
+  constexpr bool PO = std::is_same_v<Op, OpPoisson2D>;
+  constexpr int V = 4;
+  constexpr int HX = (T + 3) / 4 * 4;
+  constexpr int RPBX = kStream2dWidth - 2 * HX;
+  const int lane = threadIdx.x & 31;
+  const int ny = p.L.n1;
+  const int64_t sy = p.L.sy;
+  const int gx = strip * RPBX - HX + V * lane;  // multiple of 4
+  // n0 % 4 == 0: the lane's four cells are all inside or all outside
+  const bool xin = (unsigned)gx < (unsigned)p.L.n0;
+  const uint32_t lmask = xin ? ~0u : 0u;
+  const bool wx = V * lane >= HX && V * lane < HX + RPBX;
+  const int ys = seg * p.zseg;
+  const int ye = min(ny, ys + p.zseg);
+  const int kb = ys - T;
+  const int nit = (ye + T - 1) - kb + 1;
+  // Jacobi: coef * sum; Poisson: (sum + (-h^2) f) * 0.25
+  const float coef = PO ? 0.25f : p.op.coef;
+  const uint64_t coef2 = p2_make(coef, coef);
+  const uint64_t nh2 = p2_make(-p.op.h2, -p.op.h2);
+
+  // one row of four cells as the pairs (v0, v2), (v1, v3); zeros outside
+  auto load_pairs = [&](const float* base, int k, uint64_t& a0, uint64_t& a1, auto ld) {
+    a0 = a1 = 0ull;
+    if (xin && (unsigned)k < (unsigned)ny) {
+      const float4* src = reinterpret_cast<const float4*>(base + (int64_t)k * sy + gx);
+      const float4 a = decltype(ld)::value == kLoadCg ? __ldcg(src) : __ldg(src);
+      a0 = p2_make(a.x, a.z);
+      a1 = p2_make(a.y, a.w);
+    }
+  };
+  using LdIn = std::integral_constant<int, LD>;
+  using LdRo = std::integral_constant<int, kLoadLdg>;  // f: read-only for the whole run
+
+  uint64_t R[T][3][2];  // level t (0 = input): three newest rows, as pairs
+#pragma unroll
+  for (int t = 0; t < T; ++t)
+#pragma unroll
+    for (int s = 0; s < 3; ++s) R[t][s][0] = R[t][s][1] = 0ull;
+  uint64_t P[3][2];  // prefetched input rows k .. k+2
+#pragma unroll
+  for (int j = 0; j < 3; ++j) load_pairs(p.in, kb + j, P[j][0], P[j][1], LdIn{});
+
+  auto step = [&](auto ph, int r) {
+    constexpr int PH = decltype(ph)::value;
+    constexpr int SN = PH, SC = (PH + 2) % 3, SM = (PH + 1) % 3;  // newest, centre, y-1
+    const int k = kb + r;
+    R[0][SN][0] = P[PH][0];
+    R[0][SN][1] = P[PH][1];
+    load_pairs(p.in, k + 3, P[PH][0], P[PH][1], LdIn{});
+#pragma unroll
+    for (int t = 1; t <= T; ++t) {
+      const int q = k - t;
+      const uint64_t c0 = R[t - 1][SC][0], c1 = R[t - 1][SC][1];
+      const uint64_t m0 = R[t - 1][SM][0], m1 = R[t - 1][SM][1];  // row y-1
+      const uint64_t n0 = R[t - 1][SN][0], n1 = R[t - 1][SN][1];  // row y+1
+      const float v0 = p2_lo(c0), v2 = p2_hi(c0), v1 = p2_lo(c1);
+      const float left = __shfl_up_sync(0xffffffffu, p2_hi(c1), 1);  // v-1
+      const float right = __shfl_down_sync(0xffffffffu, v0, 1);      // v4
+      uint64_t s0, s1;
+      if constexpr (PO) {
+        // y-1, x-1, x+1, y+1 (OpPoisson2D::star2d)
+        s0 = p2_add(p2_make(p2_lo(m0) + left, p2_hi(m0) + v1), c1);
+        s0 = p2_add(s0, n0);
+        const uint64_t u = p2_add(m1, c0);
+        s1 = p2_add(p2_make(p2_lo(u) + v2, p2_hi(u) + right), n1);
+      } else {
+        // x-1, c, x+1, y-1, y+1 (OpJacobi2D::star2d)
+        s0 = p2_add(p2_make(left + v0, v1 + v2), c1);
+        const uint64_t u = p2_add(c0, c1);
+        s1 = p2_make(p2_lo(u) + v2, p2_hi(u) + right);
+        s0 = p2_add(p2_add(s0, m0), n0);
+        s1 = p2_add(p2_add(s1, m1), n1);
+      }
+      const bool qin = (unsigned)q < (unsigned)ny;
+      const uint32_t m = qin ? lmask : 0u;
+      if constexpr (PO) {  // s + (-h^2) f, the product masked before the add
+        uint64_t f0, f1;
+        load_pairs(p.aux, q, f0, f1, LdRo{});
+        s0 = p2_add(s0, p2_and(p2_mul(nh2, f0), m));
+        s1 = p2_add(s1, p2_and(p2_mul(nh2, f1), m));
+      }
+      if (t < T) {
+        R[t][SN][0] = p2_and(p2_mul(coef2, s0), m);
+        R[t][SN][1] = p2_and(p2_mul(coef2, s1), m);
+      } else if (q >= ys && q < ye && wx && xin) {
+        *reinterpret_cast<float4*>(p.out + (int64_t)q * sy + gx) =
+            make_float4(coef * p2_lo(s0), coef * p2_lo(s1), coef * p2_hi(s0), coef * p2_hi(s1));
+      }
+    }
+  };
+
+  int r = 0;
+  for (; r + 2 < nit; r += 3) {
+    step(Phase2<0>{}, r);
+    step(Phase2<1>{}, r + 1);
+    step(Phase2<2>{}, r + 2);
+  }
+  if (r < nit) step(Phase2<0>{}, r++);
+  if (r < nit) step(Phase2<1>{}, r++);
+}
+
+template <class Op, int T>
+__global__ void __launch_bounds__(kStream2dThreads)
+    stream2dp_kernel(const __grid_constant__ Stream2dParams p) {
+  grid_dependency_wait();  // no early trigger: see grid_dependency_sync
+  const int w = blockIdx.x * (kStream2dThreads / 32) + (threadIdx.x >> 5);
+  if (w >= p.ntx * p.nseg) return;  // whole warps only
+  stream2dp_body<Op, T, kLoadLdg>(p, w % p.ntx, w / p.ntx);
 }
 
 // ------------------------------------------------------------------------

@@ -134,13 +134,15 @@ typedef struct ots_params {
                                   cluster shares one tile of cluster_y * block_y
                                   * E rows, so the 2T-row y halo is recomputed
                                   once per cluster instead of once per CTA. */
-  int32_t stream_impl;         /* 3D stream kernel implementation: 0 = the
-                                  packed-FP32 kernel where it applies (jacobi-3d
-                                  and poisson-3d, T <= 4, no clusters, n a
-                                  multiple of 4, the block shapes 16x16, 16x8,
-                                  8x16 at E = 4 and 16x32, 32x16, 16x16 at
-                                  E = 2), else the scalar one; 1 = always the
-                                  scalar kernel.  Both give identical bits. */
+  int32_t stream_impl;         /* stream kernel arithmetic: 0 = the packed-FP32
+                                  kernels where they apply -- 3D: jacobi-3d and
+                                  poisson-3d, T <= 4, no clusters, n a multiple
+                                  of 4, the block shapes 16x16, 16x8, 8x16 at
+                                  E = 4 and 16x32, 32x16, 16x16 at E = 2; 2D:
+                                  jacobi-2d and poisson-2d (baseline), n a
+                                  multiple of 4 -- else the scalar ones; 1 =
+                                  always the scalar kernels.  Both give
+                                  identical bits. */
   int32_t reserved[5];         /* must be zero */
 } ots_params;
 
