@@ -44,6 +44,15 @@ __device__ __forceinline__ uint64_t p2_and(uint64_t a, uint32_t m) {
       : "l"(a), "r"(m));
   return d;
 }
+// the low half ANDed with mlo, the high half with mhi
+__device__ __forceinline__ uint64_t p2_and2(uint64_t a, uint32_t mlo, uint32_t mhi) {
+  uint64_t d;
+  asm("{.reg .b32 l, h; mov.b64 {l, h}, %1; and.b32 l, l, %2; and.b32 h, h, %3;"
+      " mov.b64 %0, {l, h};}"
+      : "=l"(d)
+      : "l"(a), "r"(mlo), "r"(mhi));
+  return d;
+}
 // 16 bytes of shared memory as two pairs, and back
 __device__ __forceinline__ void p2_lds(const float* a, uint64_t& x, uint64_t& y) {
   const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(a);

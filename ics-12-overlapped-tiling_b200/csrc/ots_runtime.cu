@@ -402,10 +402,9 @@ ots_status derive_stream2d(const ots_plan* pl, int T, Stream2dCfg* c) {
   c->rpbx = ots::kStream2dWidth - 2 * c->hx;
   const int n = pl->geo.real_size;
   c->ntx = ceil_div(n, c->rpbx);
-  // the packed form needs n0 % 4 == 0 (a lane's four cells all inside or all
-  // outside); stream_impl 1 keeps the scalar kernel
-  c->packed = !c->generic && pl->prm.stream_impl != 1 && n % 4 == 0 &&
-              pl->K->stream2dp[T] != nullptr;
+  // the packed form where the op has one (any row width); stream_impl 1
+  // keeps the scalar kernel
+  c->packed = !c->generic && pl->prm.stream_impl != 1 && pl->K->stream2dp[T] != nullptr;
   int blocks = 0;
   const bool fast = pl->prm.variant == OTS_VARIANT_FAST;
   cudaError_t oe = cudaErrorInvalidValue;

@@ -229,18 +229,19 @@ __global__ void __launch_bounds__(kStream2dThreads)
 // kernel (ots_stream3p.cuh): each add.rn.f32x2 / mul.rn.f32x2 does two IEEE
 // operations, bit for bit the scalar ones, in the op's operand order; the
 // adds that take a shuffled x neighbour (v-1 or v4) run scalar into the halves
-// of a new pair.  Requires n0 % 4 == 0 (the host runs the scalar kernel
-// otherwise), so a lane's four cells are all inside the domain or all
-// outside: the zero ring is one 32-bit AND per pair half and level, all ones
-// or zero -- and that AND between a level's multiply and the next level's
-// adds also keeps the two from being fused into one rounding.  Level T's
-// multiply is scalar, so its results land in natural x order for one 16-byte
-// store.
+// of a new pair.  The zero ring is one 32-bit AND per pair half and level --
+// and that AND between a level's multiply and the next level's adds also
+// keeps the two from being fused into one rounding.  With n0 % 4 == 0 a
+// lane's four cells are all inside the domain or all outside, so one mask
+// serves both halves; otherwise (EDGE) each half has its own, the edge lane's
+// input cells beyond n0 are cleared on load and its cells are stored one by
+// one.  Level T's multiply is scalar, so its results land in natural x order
+// for one 16-byte store.
 template <class Op>
 struct Packed2D
     : std::bool_constant<std::is_same_v<Op, OpJacobi2D> || std::is_same_v<Op, OpPoisson2D>> {};
 
-template <class Op, int T, int LD>
+template <class Op, int T, int LD, bool EDGE>
 __device__ __forceinline__ void stream2dp_body(const Stream2dParams& p, int strip, int seg) {
   static_assert(Packed2D<Op>::value, "packed form written for Jacobi-2D and Poisson-2D");
   constexpr bool PO = std::is_same_v<Op, OpPoisson2D>;
@@ -251,9 +252,15 @@ __device__ __forceinline__ void stream2dp_body(const Stream2dParams& p, int stri
   const int ny = p.L.n1;
   const int64_t sy = p.L.sy;
   const int gx = strip * RPBX - HX + V * lane;  // multiple of 4
-  // n0 % 4 == 0: the lane's four cells are all inside or all outside
-  const bool xin = (unsigned)gx < (unsigned)p.L.n0;
-  const uint32_t lmask = xin ? ~0u : 0u;
+  // the lane's cells inside the domain in x: v < kx (all four, or none,
+  // when n0 % 4 == 0); a lane left of the domain (gx < 0, a multiple of 4)
+  // has none
+  const int kx = gx < 0 ? 0 : p.L.n0 - gx;
+  const bool xin = kx > 0;
+  const bool xfull = kx >= 4;
+  // per pair half: (v0, v2) and (v1, v3)
+  const uint32_t mx00 = kx > 0 ? ~0u : 0u, mx02 = kx > 2 ? ~0u : 0u;
+  const uint32_t mx11 = kx > 1 ? ~0u : 0u, mx13 = kx > 3 ? ~0u : 0u;
   const bool wx = V * lane >= HX && V * lane < HX + RPBX;
   const int ys = seg * p.zseg;
   const int ye = min(ny, ys + p.zseg);
@@ -272,6 +279,10 @@ __device__ __forceinline__ void stream2dp_body(const Stream2dParams& p, int stri
       const float4 a = decltype(ld)::value == kLoadCg ? __ldcg(src) : __ldg(src);
       a0 = p2_make(a.x, a.z);
       a1 = p2_make(a.y, a.w);
+      if constexpr (EDGE) {  // cells beyond n0 (the row's padding) read as zero
+        a0 = p2_and2(a0, mx00, mx02);
+        a1 = p2_and2(a1, mx11, mx13);
+      }
     }
   };
   using LdIn = std::integral_constant<int, LD>;
@@ -318,19 +329,30 @@ __device__ __forceinline__ void stream2dp_body(const Stream2dParams& p, int stri
         s1 = p2_add(p2_add(s1, m1), n1);
       }
       const bool qin = (unsigned)q < (unsigned)ny;
-      const uint32_t m = qin ? lmask : 0u;
+      const uint32_t mq = qin ? ~0u : 0u;
+      // the zero-ring masks of this level: (v0, v2) and (v1, v3)
+      const uint32_t m00 = EDGE ? (mq & mx00) : (mq & mx13), m02 = EDGE ? (mq & mx02) : m00;
+      const uint32_t m11 = EDGE ? (mq & mx11) : m00, m13 = EDGE ? (mq & mx13) : m00;
       if constexpr (PO) {  // s + (-h^2) f, the product masked before the add
         uint64_t f0, f1;
         load_pairs(p.aux, q, f0, f1, LdRo{});
-        s0 = p2_add(s0, p2_and(p2_mul(nh2, f0), m));
-        s1 = p2_add(s1, p2_and(p2_mul(nh2, f1), m));
+        s0 = p2_add(s0, p2_and2(p2_mul(nh2, f0), m00, m02));
+        s1 = p2_add(s1, p2_and2(p2_mul(nh2, f1), m11, m13));
       }
       if (t < T) {
-        R[t][SN][0] = p2_and(p2_mul(coef2, s0), m);
-        R[t][SN][1] = p2_and(p2_mul(coef2, s1), m);
+        R[t][SN][0] = p2_and2(p2_mul(coef2, s0), m00, m02);
+        R[t][SN][1] = p2_and2(p2_mul(coef2, s1), m11, m13);
       } else if (q >= ys && q < ye && wx && xin) {
-        *reinterpret_cast<float4*>(p.out + (int64_t)q * sy + gx) =
+        const float4 o =
             make_float4(coef * p2_lo(s0), coef * p2_lo(s1), coef * p2_hi(s0), coef * p2_hi(s1));
+        float* const dst = p.out + (int64_t)q * sy + gx;
+        if (!EDGE || xfull) {
+          *reinterpret_cast<float4*>(dst) = o;
+        } else {  // the edge lane: its cells inside the domain only
+          dst[0] = o.x;
+          if (kx > 1) dst[1] = o.y;
+          if (kx > 2) dst[2] = o.z;
+        }
       }
     }
   };
@@ -351,7 +373,10 @@ __global__ void __launch_bounds__(kStream2dThreads)
   grid_dependency_wait();  // no early trigger: see grid_dependency_sync
   const int w = blockIdx.x * (kStream2dThreads / 32) + (threadIdx.x >> 5);
   if (w >= p.ntx * p.nseg) return;  // whole warps only
-  stream2dp_body<Op, T, kLoadLdg>(p, w % p.ntx, w / p.ntx);
+  if (p.L.n0 % 4 == 0)
+    stream2dp_body<Op, T, kLoadLdg, false>(p, w % p.ntx, w / p.ntx);
+  else
+    stream2dp_body<Op, T, kLoadLdg, true>(p, w % p.ntx, w / p.ntx);
 }
 
 // ------------------------------------------------------------------------

@@ -268,29 +268,28 @@ def test_stream2d_kernel_matches_oracle(st, T):
 @pytest.mark.parametrize("st", ["jacobi-2d", "poisson-2d"])
 @pytest.mark.parametrize("T", [1, 2, 3, 4, 5, 8])
 def test_stream2d_packed_kernel_matches_oracle(st, T):
-    # the packed-FP32 form (n % 4 == 0): bit for bit against the oracle and
+    # the packed-FP32 form, n a multiple of 4 (one mask per lane) and not (the
+    # edge lane's cells masked one by one): bit for bit against the oracle and
     # against the scalar kernel (stream_impl 1), n not a multiple of the strip
     # interior, several y segments, the last launch shallower than T
-    outs = []
-    for impl in (0, 1):
-        with ots.Plan(st, 300, 2 * T + 1, T=T, bx=32, by=1, E=1, kernel="stream",
-                      impl=impl) as plan:
-            assert plan.describe()["Stream Arithmetic"] == ("packed-fp32" if impl == 0
-                                                            else "scalar")
-            g = plan.geometry
-            state, aux = inputs(plan, seed=31 + T)
-            plan.upload(state, aux)
-            plan.run()
-            outs.append(plan.download()[0])
-    want = O.sweep_f32(st, state, aux=aux, steps=2 * T + 1, lo=g.padding,
-                       hi=g.padding + g.real_size, coef=g.coef, h2=g.h2)[0]
-    for o in outs:
-        assert np.array_equal(o.view(np.uint32), want.view(np.uint32))
-    # n % 4 != 0 runs the scalar kernel
-    with ots.Plan(st, 301, 3, T=T, bx=32, by=1, E=1, kernel="stream") as plan:
-        assert plan.describe()["Stream Arithmetic"] == "scalar"
+    for n in (300, 301, 302, 303):
+        outs = []
+        for impl in (0, 1):
+            with ots.Plan(st, n, 2 * T + 1, T=T, bx=32, by=1, E=1, kernel="stream",
+                          impl=impl) as plan:
+                assert plan.describe()["Stream Arithmetic"] == ("packed-fp32" if impl == 0
+                                                                else "scalar")
+                g = plan.geometry
+                state, aux = inputs(plan, seed=31 + T)
+                plan.upload(state, aux)
+                plan.run()
+                outs.append(plan.download()[0])
+        want = O.sweep_f32(st, state, aux=aux, steps=2 * T + 1, lo=g.padding,
+                           hi=g.padding + g.real_size, coef=g.coef, h2=g.h2)[0]
+        for o in outs:
+            assert np.array_equal(o.view(np.uint32), want.view(np.uint32)), n
     # edge sizes: a single strip, one row per segment, the reference weight
-    for n, steps, by in ((4, 3, 1), (128, 9, 1), (240, 7, 16)):
+    for n, steps, by in ((4, 3, 1), (5, 3, 1), (128, 9, 1), (129, 7, 1), (240, 7, 16)):
         run_and_check(st, n, steps, T=T, bx=32, by=by, bz=1, E=1, kernel="stream")
     if st == "jacobi-2d":
         run_and_check(st, 64, 5, T=T, bx=32, by=1, bz=1, E=1, kernel="stream",
