@@ -296,6 +296,13 @@ __device__ __forceinline__ void stream2dp_body(const Stream2dParams& p, int stri
   uint64_t P[3][2];  // prefetched input rows k .. k+2
 #pragma unroll
   for (int j = 0; j < 3; ++j) load_pairs(p.in, kb + j, P[j][0], P[j][1], LdIn{});
+  // Poisson: level t's f row of the coming iteration, fetched one iteration
+  // ahead (a load issued where it is used stalls the level on L2)
+  uint64_t Fq[PO ? T : 1][2];
+  if constexpr (PO) {
+#pragma unroll
+    for (int t = 1; t <= T; ++t) load_pairs(p.aux, kb - t, Fq[t - 1][0], Fq[t - 1][1], LdRo{});
+  }
 
   auto step = [&](auto ph, int r) {
     constexpr int PH = decltype(ph)::value;
@@ -334,10 +341,9 @@ __device__ __forceinline__ void stream2dp_body(const Stream2dParams& p, int stri
       const uint32_t m00 = EDGE ? (mq & mx00) : (mq & mx13), m02 = EDGE ? (mq & mx02) : m00;
       const uint32_t m11 = EDGE ? (mq & mx11) : m00, m13 = EDGE ? (mq & mx13) : m00;
       if constexpr (PO) {  // s + (-h^2) f, the product masked before the add
-        uint64_t f0, f1;
-        load_pairs(p.aux, q, f0, f1, LdRo{});
-        s0 = p2_add(s0, p2_and2(p2_mul(nh2, f0), m00, m02));
-        s1 = p2_add(s1, p2_and2(p2_mul(nh2, f1), m11, m13));
+        s0 = p2_add(s0, p2_and2(p2_mul(nh2, Fq[t - 1][0]), m00, m02));
+        s1 = p2_add(s1, p2_and2(p2_mul(nh2, Fq[t - 1][1]), m11, m13));
+        load_pairs(p.aux, q + 1, Fq[t - 1][0], Fq[t - 1][1], LdRo{});
       }
       if (t < T) {
         R[t][SN][0] = p2_and2(p2_mul(coef2, s0), m00, m02);
