@@ -404,12 +404,13 @@ ots_status derive_stream2d(const ots_plan* pl, int T, Stream2dCfg* c) {
   c->ntx = ceil_div(n, c->rpbx);
   // the packed form where the op has one (any row width); stream_impl 1
   // keeps the scalar kernel
-  c->packed = !c->generic && pl->prm.stream_impl != 1 && pl->K->stream2dp[T] != nullptr;
+  c->packed = pl->prm.stream_impl != 1 &&
+              (c->generic ? pl->prm.stencil == OTS_FDTD_2D : pl->K->stream2dp[T] != nullptr);
   int blocks = 0;
   const bool fast = pl->prm.variant == OTS_VARIANT_FAST;
   cudaError_t oe = cudaErrorInvalidValue;
   if (c->generic && pl->K->stream2dg_occ[T])
-    oe = pl->K->stream2dg_occ[T](&blocks, fast);
+    oe = pl->K->stream2dg_occ[T](&blocks, fast, !c->packed);
   else if (c->packed && pl->K->stream2dp_occ[T])
     oe = pl->K->stream2dp_occ[T](&blocks);
   else if (!c->generic && pl->K->stream2d_occ[T])
@@ -678,7 +679,7 @@ void fill_geometry_for_kernel(ots_plan* pl) {
     }
     if (c.generic) {
       auto attr = pl->K->stream2dg_attr[c.T];
-      if (attr && attr(&a, pl->prm.variant == OTS_VARIANT_FAST) == cudaSuccess)
+      if (attr && attr(&a, pl->prm.variant == OTS_VARIANT_FAST, !c.packed) == cudaSuccess)
         g.registers = a.numRegs;
     } else {
       auto attr = c.packed ? pl->K->stream2dp_attr[c.T] : pl->K->stream2d_attr[c.T];
@@ -831,6 +832,7 @@ ots_status enqueue_run(ots_plan* pl, int kernel) {
         sp.zseg = c.zseg;
         sp.base_step = base;
         sp.op = pl->op;
+        sp.impl = c.packed ? 0 : 1;
         e = pl->K->stream2dg[Tl](sp, dim3(c.grid), pl->stream);
       } else {
         ots::Stream2dParams sp{};
