@@ -51,6 +51,8 @@ void usage(const char* prog) {
           "      --kernel auto|tile|stream|plain|tex\n"
           "      --variant ref|baseline|fast  Arithmetic variant (default: ref for compat;\n"
           "                               fast: approximate division, rician / tv / cs-3d)\n"
+          "      --stream-impl N          Stream kernels' arithmetic: 0 packed FP32 where it\n"
+          "                               applies (default), 1 scalar, 2 also fdtd-2d packed\n"
           "      --coef X                 Averaging weight (Jacobi stencils)\n"
           "      --seed N                 srand seed for the input fill (default 123456)\n"
           "      --init ref|baseline      Inputs: the reference fill everywhere (default), or the\n"
@@ -207,7 +209,8 @@ int main(int argc, char** argv) {
       p.variant = strcmp(v, "baseline") == 0 ? OTS_VARIANT_BASELINE
                   : strcmp(v, "fast") == 0   ? OTS_VARIANT_FAST
                                              : OTS_VARIANT_REF;
-    } else if (a == "--coef") p.coef = (float)atof(next());
+    } else if (a == "--stream-impl") p.stream_impl = atoi(next());
+    else if (a == "--coef") p.coef = (float)atof(next());
     else if (a == "--seed") seed = (unsigned)strtoul(next(), nullptr, 10);
     else if (a == "--init") init_baseline = strcmp(next(), "baseline") == 0;
     else if (a == "--plain") plain = true;

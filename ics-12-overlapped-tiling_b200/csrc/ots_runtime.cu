@@ -243,8 +243,9 @@ ots_status derive(const ots_params* p, ots_geometry* g, const StencilInfo** info
     return fail(OTS_ERR_INVALID_ARGUMENT, "unknown stencil id %d", p->stencil);
   for (int i = 0; i < 5; ++i)
     if (p->reserved[i] != 0) return fail(OTS_ERR_INVALID_ARGUMENT, "reserved fields must be 0");
-  if (p->stream_impl < 0 || p->stream_impl > 1)
-    return fail(OTS_ERR_INVALID_ARGUMENT, "stream_impl must be 0 or 1 (got %d)", p->stream_impl);
+  if (p->stream_impl < 0 || p->stream_impl > 2)
+    return fail(OTS_ERR_INVALID_ARGUMENT, "stream_impl must be 0, 1 or 2 (got %d)",
+                p->stream_impl);
   if (p->cluster_y < 0 || p->cluster_y > 8)
     return fail(OTS_ERR_INVALID_ARGUMENT, "cluster_y must be 0..8 (got %d)", p->cluster_y);
   const StencilInfo& si = kInfo[p->stencil];
@@ -403,9 +404,10 @@ ots_status derive_stream2d(const ots_plan* pl, int T, Stream2dCfg* c) {
   const int n = pl->geo.real_size;
   c->ntx = ceil_div(n, c->rpbx);
   // the packed form where the op has one (any row width); stream_impl 1
-  // keeps the scalar kernel
-  c->packed = pl->prm.stream_impl != 1 &&
-              (c->generic ? pl->prm.stencil == OTS_FDTD_2D : pl->K->stream2dp[T] != nullptr);
+  // keeps the scalar kernel.  FDTD's packed kernel only when asked for
+  // (stream_impl 2): it is faster than the scalar one at T = 6 alone.
+  c->packed = c->generic ? pl->prm.stencil == OTS_FDTD_2D && pl->prm.stream_impl == 2
+                         : pl->prm.stream_impl != 1 && pl->K->stream2dp[T] != nullptr;
   int blocks = 0;
   const bool fast = pl->prm.variant == OTS_VARIANT_FAST;
   cudaError_t oe = cudaErrorInvalidValue;

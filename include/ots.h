@@ -139,11 +139,11 @@ typedef struct ots_params {
                                   poisson-3d, T <= 4, no clusters, n a multiple
                                   of 4, the block shapes 16x16, 16x8, 8x16 at
                                   E = 4 and 16x32, 32x16, 16x16 at E = 2; 2D:
-                                  jacobi-2d, poisson-2d (baseline) and
-                                  fdtd-2d -- else
-                                  the scalar ones; 1 =
-                                  always the scalar kernels.  Both give
-                                  identical bits. */
+                                  jacobi-2d and poisson-2d (baseline) -- else
+                                  the scalar ones; 1 = always the scalar
+                                  kernels; 2 = as 0, and fdtd-2d's packed
+                                  kernel too (faster than its scalar one at
+                                  T = 6 only).  All give identical bits. */
   int32_t reserved[5];         /* must be zero */
 } ots_params;
 
