@@ -401,8 +401,8 @@ ots_status ots_mlp_topk(ots_mlp* model, const float* X, int32_t n, int32_t k, in
  *     at most 4096 rows per call, and every layer at most 64 wide; larger
  *     requests are rejected with OTS_ERR_INVALID_ARGUMENT / UNSUPPORTED.
  *   - The first call on each device looks up that array's device address
- *     (cudaGetSymbolAddress) with the model's device current; make that first
- *     call before any stream capture.
+ *     (cudaGetSymbolAddress) with the model's device current, and later calls
+ *     reuse it.
  *   - All calls share the array: calls whose work overlaps on the GPU race
  *     (serialise them on one stream).  Each call overwrites what it reads,
  *     so nothing carries over from the previous call.
