@@ -41,9 +41,8 @@ constexpr int kStream1dVs[3] = {4, 8, 16};  // cells per lane of the 1D register
 using Occ2dFn = cudaError_t (*)(int*);
 // the generic 2D stream kernels: `fast` selects the fast-division
 // instantiation where an op has one (Rician)
-// (and `scalar` the scalar FDTD kernel instead of its packed form)
-using Occ2dgFn = cudaError_t (*)(int*, bool fast, bool scalar);
-using Attr2dgFn = cudaError_t (*)(cudaFuncAttributes*, bool fast, bool scalar);
+using Occ2dgFn = cudaError_t (*)(int*, bool fast);
+using Attr2dgFn = cudaError_t (*)(cudaFuncAttributes*, bool fast);
 // stream kernel queries take the cluster flag (the clustered instantiation)
 using StreamAttrFn = cudaError_t (*)(cudaFuncAttributes*, bool);
 using StreamOccFn = cudaError_t (*)(int*, int, size_t, bool);
@@ -293,15 +292,14 @@ cudaError_t attr_stream1d(cudaFuncAttributes* a) {
 }
 
 // The y-streamed kernel of a stencil without the five-point form: FDTD-2D
-// and Rician-denoise-2D have their own two-phase kernels (FDTD's packed-FP32
-// form unless `scalar`; Rician's in two instantiations, IEEE and fast
-// division: `fast` picks one); every other op goes through its apply().
+// and Rician-denoise-2D have their own two-phase kernels (Rician's in two
+// instantiations, IEEE and fast division: `fast` picks one); every other op
+// goes through its apply().
 template <class Op, int T>
-auto stream2dg_entry(bool fast = false, bool scalar = false) {
+auto stream2dg_entry(bool fast = false) {
   (void)fast;
-  (void)scalar;
   if constexpr (std::is_same_v<Op, OpFdtd2D>)
-    return scalar ? &stream2d_fdtd_kernel<T> : &stream2dp_fdtd_kernel<T>;
+    return &stream2d_fdtd_kernel<T>;
   else if constexpr (std::is_same_v<Op, OpRician2D>)
     return fast ? &stream2d_rician_kernel<T, true> : &stream2d_rician_kernel<T, false>;
   else
@@ -310,18 +308,18 @@ auto stream2dg_entry(bool fast = false, bool scalar = false) {
 
 template <class Op, int T>
 cudaError_t launch_stream2dg(const Stream2dgParams& p, dim3 g, cudaStream_t s) {
-  return launch_k(stream2dg_entry<Op, T>(p.op.variant == 2, p.impl == 1), g,
-                  dim3(kStream2dThreads), 0, s, 1, p);
+  return launch_k(stream2dg_entry<Op, T>(p.op.variant == 2), g, dim3(kStream2dThreads), 0, s, 1,
+                  p);
 }
 
 template <class Op, int T>
-cudaError_t attr_stream2dg(cudaFuncAttributes* a, bool fast, bool scalar) {
-  return cudaFuncGetAttributes(a, stream2dg_entry<Op, T>(fast, scalar));
+cudaError_t attr_stream2dg(cudaFuncAttributes* a, bool fast) {
+  return cudaFuncGetAttributes(a, stream2dg_entry<Op, T>(fast));
 }
 
 template <class Op, int T>
-cudaError_t occ_stream2dg(int* blocks, bool fast, bool scalar) {
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, stream2dg_entry<Op, T>(fast, scalar),
+cudaError_t occ_stream2dg(int* blocks, bool fast) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, stream2dg_entry<Op, T>(fast),
                                                        kStream2dThreads, 0);
 }
 

@@ -52,7 +52,7 @@ void usage(const char* prog) {
           "      --variant ref|baseline|fast  Arithmetic variant (default: ref for compat;\n"
           "                               fast: approximate division, rician / tv / cs-3d)\n"
           "      --stream-impl N          Stream kernels' arithmetic: 0 packed FP32 where it\n"
-          "                               applies (default), 1 scalar, 2 also fdtd-2d packed\n"
+          "                               applies (default), 1 scalar\n"
           "      --coef X                 Averaging weight (Jacobi stencils)\n"
           "      --seed N                 srand seed for the input fill (default 123456)\n"
           "      --init ref|baseline      Inputs: the reference fill everywhere (default), or the\n"

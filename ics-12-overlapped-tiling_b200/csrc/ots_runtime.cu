@@ -243,9 +243,8 @@ ots_status derive(const ots_params* p, ots_geometry* g, const StencilInfo** info
     return fail(OTS_ERR_INVALID_ARGUMENT, "unknown stencil id %d", p->stencil);
   for (int i = 0; i < 5; ++i)
     if (p->reserved[i] != 0) return fail(OTS_ERR_INVALID_ARGUMENT, "reserved fields must be 0");
-  if (p->stream_impl < 0 || p->stream_impl > 2)
-    return fail(OTS_ERR_INVALID_ARGUMENT, "stream_impl must be 0, 1 or 2 (got %d)",
-                p->stream_impl);
+  if (p->stream_impl < 0 || p->stream_impl > 1)
+    return fail(OTS_ERR_INVALID_ARGUMENT, "stream_impl must be 0 or 1 (got %d)", p->stream_impl);
   if (p->cluster_y < 0 || p->cluster_y > 8)
     return fail(OTS_ERR_INVALID_ARGUMENT, "cluster_y must be 0..8 (got %d)", p->cluster_y);
   const StencilInfo& si = kInfo[p->stencil];
@@ -404,15 +403,13 @@ ots_status derive_stream2d(const ots_plan* pl, int T, Stream2dCfg* c) {
   const int n = pl->geo.real_size;
   c->ntx = ceil_div(n, c->rpbx);
   // the packed form where the op has one (any row width); stream_impl 1
-  // keeps the scalar kernel.  FDTD's packed kernel only when asked for
-  // (stream_impl 2): it is faster than the scalar one at T = 6 alone.
-  c->packed = c->generic ? pl->prm.stencil == OTS_FDTD_2D && pl->prm.stream_impl == 2
-                         : pl->prm.stream_impl != 1 && pl->K->stream2dp[T] != nullptr;
+  // keeps the scalar kernel
+  c->packed = !c->generic && pl->prm.stream_impl != 1 && pl->K->stream2dp[T] != nullptr;
   int blocks = 0;
   const bool fast = pl->prm.variant == OTS_VARIANT_FAST;
   cudaError_t oe = cudaErrorInvalidValue;
   if (c->generic && pl->K->stream2dg_occ[T])
-    oe = pl->K->stream2dg_occ[T](&blocks, fast, !c->packed);
+    oe = pl->K->stream2dg_occ[T](&blocks, fast);
   else if (c->packed && pl->K->stream2dp_occ[T])
     oe = pl->K->stream2dp_occ[T](&blocks);
   else if (!c->generic && pl->K->stream2d_occ[T])
@@ -681,7 +678,7 @@ void fill_geometry_for_kernel(ots_plan* pl) {
     }
     if (c.generic) {
       auto attr = pl->K->stream2dg_attr[c.T];
-      if (attr && attr(&a, pl->prm.variant == OTS_VARIANT_FAST, !c.packed) == cudaSuccess)
+      if (attr && attr(&a, pl->prm.variant == OTS_VARIANT_FAST) == cudaSuccess)
         g.registers = a.numRegs;
     } else {
       auto attr = c.packed ? pl->K->stream2dp_attr[c.T] : pl->K->stream2d_attr[c.T];
@@ -834,7 +831,6 @@ ots_status enqueue_run(ots_plan* pl, int kernel) {
         sp.zseg = c.zseg;
         sp.base_step = base;
         sp.op = pl->op;
-        sp.impl = c.packed ? 0 : 1;
         e = pl->K->stream2dg[Tl](sp, dim3(c.grid), pl->stream);
       } else {
         ots::Stream2dParams sp{};

@@ -413,7 +413,6 @@ struct Stream2dgParams {
   Layout L;
   int ntx, nseg, zseg, base_step;
   OpArgs op;
-  int impl;  // 1: the scalar FDTD kernel instead of the packed one
 };
 
 template <int NS, int D, int RX, int PH, int R>
@@ -662,8 +661,11 @@ __global__ void __launch_bounds__(kStream2dThreads)
 #pragma unroll
     for (int f = 0; f < 3; ++f) load4(p.in[f], kb + j, Pf[j][f]);
 
-  auto step = [&](auto ph, int r) {
+  // EDG: some level's row of this iteration may lie outside [0, ny) and is
+  // zeroed; otherwise every level's rows are inside and only x is tested
+  auto step = [&](auto ph, auto edg, int r) {
     constexpr int PH = decltype(ph)::value, PO = PH ^ 1;
+    constexpr bool EDG = decltype(edg)::value != 0;
     const int k = kb + r;
 #pragma unroll
     for (int f = 0; f < 3; ++f) {
@@ -682,7 +684,7 @@ __global__ void __launch_bounds__(kStream2dThreads)
       const int step_t = p.base_step + t - 1;
       // E' of row qE (OpFdtd2D::ex_new / ey_new at that row)
       const float hl = __shfl_up_sync(0xffffffffu, Lh[V - 1], 1);  // Hz(qE) at x - 1 of cell 0
-      const bool qEin = (unsigned)qE < (unsigned)ny;
+      const bool qEin = !EDG || (unsigned)qE < (unsigned)ny;
 #pragma unroll
       for (int v = 0; v < V; ++v) {
         const bool in = qEin && ((xin >> v) & 1);
@@ -694,7 +696,7 @@ __global__ void __launch_bounds__(kStream2dThreads)
       }
       // H' of row qH from E'(qH) (slot PO) and Ey'(qE)
       const float exr = __shfl_down_sync(0xffffffffu, Ec[t][PO][0][0], 1);  // Ex'(qH) at x + 1 of cell 3
-      const bool qHin = (unsigned)qH < (unsigned)ny;
+      const bool qHin = !EDG || (unsigned)qH < (unsigned)ny;
 #pragma unroll
       for (int v = 0; v < V; ++v) {
         const float ex = Ec[t][PO][0][v], ey = Ec[t][PO][1][v];
@@ -729,163 +731,16 @@ __global__ void __launch_bounds__(kStream2dThreads)
 
   int r = 0;
   for (; r + 1 < nit; r += 2) {
-    step(PhaseG<0>{}, r);
-    step(PhaseG<1>{}, r + 1);
+    // the two iterations' level rows span [kb + r - T, kb + r + 1]
+    if (kb + r - T >= 0 && kb + r + 1 < ny) {
+      step(PhaseG<0>{}, PhaseG<0>{}, r);
+      step(PhaseG<1>{}, PhaseG<0>{}, r + 1);
+    } else {
+      step(PhaseG<0>{}, PhaseG<1>{}, r);
+      step(PhaseG<1>{}, PhaseG<1>{}, r + 1);
+    }
   }
-  if (r < nit) step(PhaseG<0>{}, r);
-}
-
-// FDTD-2D streamed in its two phases with packed FP32 arithmetic: the kernel
-// above, each lane's four cells of each field held as the pairs (v0, v2) and
-// (v1, v3) (as in the packed Jacobi kernels), every operation in the same
-// order on the same operands -- bit for bit its results.  The differences
-// that take a shuffled x neighbour (Hz at x-1 of v0, Ex' at x+1 of v3) run
-// scalar into the halves of a new pair.  The three products 0.5 d and 0.7 d
-// are ANDed with the zero-ring mask of their row before the subtraction: the
-// AND keeps each multiply and subtraction from being fused into one rounding,
-// and since every field is zero outside the domain (input ring and every
-// level's masked products), x - 0 leaves the outside cells at +0 exactly as
-// the scalar kernel's selects do.  Any row width: each pair half has its own
-// mask, the edge lane's cells beyond n0 are cleared on load and stored one by
-// one.
-template <int T>
-__global__ void __launch_bounds__(kStream2dThreads)
-    stream2dp_fdtd_kernel(const __grid_constant__ Stream2dgParams p) {
-  constexpr int V = 4, HX = (T + 3) / 4 * 4;
-  constexpr int RPBX = kStream2dWidth - 2 * HX;
-  static_assert(RPBX >= 4, "depth");
-  grid_dependency_sync();
-  const int w = blockIdx.x * (kStream2dThreads / 32) + (threadIdx.x >> 5);
-  if (w >= p.ntx * p.nseg) return;  // whole warps only
-  const int strip = w % p.ntx, seg = w / p.ntx;
-  const int lane = threadIdx.x & 31;
-  const int ny = p.L.n1;
-  const int64_t sy = p.L.sy;
-  const int gx = strip * RPBX - HX + V * lane;  // multiple of 4
-  // cells inside the domain in x: v < kx; per pair half (v0, v2), (v1, v3)
-  const int kx = gx < 0 ? 0 : p.L.n0 - gx;
-  const bool xin = kx > 0, xfull = kx >= 4;
-  const uint32_t mx0 = kx > 0 ? ~0u : 0u, mx2 = kx > 2 ? ~0u : 0u;
-  const uint32_t mx1 = kx > 1 ? ~0u : 0u, mx3 = kx > 3 ? ~0u : 0u;
-  const bool wx = V * lane >= HX && V * lane < HX + RPBX;
-  const int ys = seg * p.zseg;
-  const int ye = min(ny, ys + p.zseg);
-  const int kb = ys - T;
-  const int nit = (ye + T - 1) - kb + 1;
-  const bool src_row = p.op.variant == 0;  // Ey on interior row 0 driven to the step index
-  const bool plus_ey = p.op.variant == 1;   // the reference's "+Ey" in the Hz update
-  const uint64_t half2 = p2_make(0.5f, 0.5f), c07 = p2_make(0.7f, 0.7f);
-
-  // one row of a field as pairs, zeros outside the domain
-  auto load2 = [&](const float* base, int k, uint64_t (&d)[2]) {
-    d[0] = d[1] = 0ull;
-    if (xin && (unsigned)k < (unsigned)ny) {
-      const float4 a = __ldg(reinterpret_cast<const float4*>(base + (int64_t)k * sy + gx));
-      d[0] = p2_and2(p2_make(a.x, a.z), mx0, mx2);
-      d[1] = p2_and2(p2_make(a.y, a.w), mx1, mx3);
-    }
-  };
-
-  uint64_t In[2][3][2];         // level 0: input rows k (slot PH) and k - 1 (slot PH ^ 1)
-  uint64_t Pf[2][3][2];         // input rows fetched ahead
-  uint64_t Ec[T + 1][2][2][2];  // level t: E' rows (slot PH: row k - t + 1; PH ^ 1: row k - t)
-  uint64_t Hl[T + 1][2][2];     // level t: H' rows (slot PH: row k - t; PH ^ 1: row k - t - 1)
-#pragma unroll
-  for (int s = 0; s < 2; ++s)
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-#pragma unroll
-      for (int f = 0; f < 3; ++f) In[s][f][h] = 0ull;
-#pragma unroll
-      for (int t = 0; t <= T; ++t) {
-        Ec[t][s][0][h] = Ec[t][s][1][h] = 0ull;
-        Hl[t][s][h] = 0ull;
-      }
-    }
-#pragma unroll
-  for (int j = 0; j < 2; ++j)
-#pragma unroll
-    for (int f = 0; f < 3; ++f) load2(p.in[f], kb + j, Pf[j][f]);
-
-  auto step = [&](auto ph, int r) {
-    constexpr int PH = decltype(ph)::value, PO = PH ^ 1;
-    const int k = kb + r;
-#pragma unroll
-    for (int f = 0; f < 3; ++f) {
-      In[PH][f][0] = Pf[PH][f][0];
-      In[PH][f][1] = Pf[PH][f][1];
-      load2(p.in[f], k + 2, Pf[PH][f]);
-    }
-#pragma unroll
-    for (int t = 1; t <= T; ++t) {
-      const int qE = k - t + 1, qH = k - t;
-      // level t-1's row qE (Ex, Ey, Hz) and its Hz of row qE - 1 = qH
-      const uint64_t(&Lx)[2] = t == 1 ? In[PH][0] : Ec[t > 1 ? t - 1 : 0][PO][0];
-      const uint64_t(&Ly)[2] = t == 1 ? In[PH][1] : Ec[t > 1 ? t - 1 : 0][PO][1];
-      const uint64_t(&Lh)[2] = t == 1 ? In[PH][2] : Hl[t > 1 ? t - 1 : 0][PH];
-      const uint64_t(&Lhp)[2] = t == 1 ? In[PO][2] : Hl[t > 1 ? t - 1 : 0][PO];
-      const int step_t = p.base_step + t - 1;
-      const uint32_t mE = (unsigned)qE < (unsigned)ny ? ~0u : 0u;
-      const uint32_t mE0 = mE & mx0, mE2 = mE & mx2, mE1 = mE & mx1, mE3 = mE & mx3;
-      // E' of row qE: Ex' = Ex - 0.5 (Hz - Hz(x-1)), Ey' = Ey - 0.5 (Hz - Hz(y-1))
-      const float hl = __shfl_up_sync(0xffffffffu, p2_hi(Lh[1]), 1);  // Hz at x-1 of v0
-      const uint64_t dx0 = p2_make(p2_lo(Lh[0]) - hl, p2_hi(Lh[0]) - p2_lo(Lh[1]));
-      const uint64_t dx1 = p2_sub(Lh[1], Lh[0]);
-      Ec[t][PH][0][0] = p2_sub(Lx[0], p2_and2(p2_mul(half2, dx0), mE0, mE2));
-      Ec[t][PH][0][1] = p2_sub(Lx[1], p2_and2(p2_mul(half2, dx1), mE1, mE3));
-      if (src_row && qE == 0) {
-        const uint64_t tt = p2_make((float)step_t, (float)step_t);
-        Ec[t][PH][1][0] = p2_and2(tt, mE0, mE2);
-        Ec[t][PH][1][1] = p2_and2(tt, mE1, mE3);
-      } else {
-        Ec[t][PH][1][0] = p2_sub(Ly[0], p2_and2(p2_mul(half2, p2_sub(Lh[0], Lhp[0])), mE0, mE2));
-        Ec[t][PH][1][1] = p2_sub(Ly[1], p2_and2(p2_mul(half2, p2_sub(Lh[1], Lhp[1])), mE1, mE3));
-      }
-      // H' of row qH from E'(qH) (slot PO) and Ey'(qE):
-      // Hz - 0.7 ((Ex'(x+1) - Ex') + Ey'(y+1) -/+ Ey')
-      const uint64_t(&ex)[2] = Ec[t][PO][0];
-      const uint64_t(&ey)[2] = Ec[t][PO][1];
-      const float exr = __shfl_down_sync(0xffffffffu, p2_lo(ex[0]), 1);  // Ex' at x+1 of v3
-      uint64_t d0 = p2_add(p2_sub(ex[1], ex[0]), Ec[t][PH][1][0]);
-      uint64_t d1 = p2_add(p2_make(p2_hi(ex[0]) - p2_lo(ex[1]), exr - p2_hi(ex[1])),
-                           Ec[t][PH][1][1]);
-      d0 = plus_ey ? p2_add(d0, ey[0]) : p2_sub(d0, ey[0]);
-      d1 = plus_ey ? p2_add(d1, ey[1]) : p2_sub(d1, ey[1]);
-      const uint32_t mH = (unsigned)qH < (unsigned)ny ? ~0u : 0u;
-      Hl[t][PH][0] = p2_sub(Lhp[0], p2_and2(p2_mul(c07, d0), mH & mx0, mH & mx2));
-      Hl[t][PH][1] = p2_sub(Lhp[1], p2_and2(p2_mul(c07, d1), mH & mx1, mH & mx3));
-      if (t == T && qH >= ys && qH < ye && wx && xin) {
-        const uint64_t(&ox)[2] = Ec[T][PO][0];
-        const uint64_t(&oy)[2] = Ec[T][PO][1];
-        const uint64_t(&oh)[2] = Hl[T][PH];
-        const float4 vx = make_float4(p2_lo(ox[0]), p2_lo(ox[1]), p2_hi(ox[0]), p2_hi(ox[1]));
-        const float4 vy = make_float4(p2_lo(oy[0]), p2_lo(oy[1]), p2_hi(oy[0]), p2_hi(oy[1]));
-        const float4 vh = make_float4(p2_lo(oh[0]), p2_lo(oh[1]), p2_hi(oh[0]), p2_hi(oh[1]));
-        float* const d[3] = {p.out[0] + (int64_t)qH * sy + gx, p.out[1] + (int64_t)qH * sy + gx,
-                             p.out[2] + (int64_t)qH * sy + gx};
-        if (xfull) {
-          *reinterpret_cast<float4*>(d[0]) = vx;
-          *reinterpret_cast<float4*>(d[1]) = vy;
-          *reinterpret_cast<float4*>(d[2]) = vh;
-        } else {  // the edge lane: its cells inside the domain only
-          const float4 v3[3] = {vx, vy, vh};
-#pragma unroll
-          for (int f = 0; f < 3; ++f) {
-            d[f][0] = v3[f].x;
-            if (kx > 1) d[f][1] = v3[f].y;
-            if (kx > 2) d[f][2] = v3[f].z;
-          }
-        }
-      }
-    }
-  };
-
-  int r = 0;
-  for (; r + 1 < nit; r += 2) {
-    step(PhaseG<0>{}, r);
-    step(PhaseG<1>{}, r + 1);
-  }
-  if (r < nit) step(PhaseG<0>{}, r);
+  if (r < nit) step(PhaseG<0>{}, PhaseG<1>{}, r);
 }
 
 // Rician-denoise-2D streamed in its two phases.  The fused update

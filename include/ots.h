@@ -141,9 +141,7 @@ typedef struct ots_params {
                                   E = 4 and 16x32, 32x16, 16x16 at E = 2; 2D:
                                   jacobi-2d and poisson-2d (baseline) -- else
                                   the scalar ones; 1 = always the scalar
-                                  kernels; 2 = as 0, and fdtd-2d's packed
-                                  kernel too (faster than its scalar one at
-                                  T = 6 only).  All give identical bits. */
+                                  kernels.  Both give identical bits. */
   int32_t reserved[5];         /* must be zero */
 } ots_params;
 

@@ -123,7 +123,7 @@ def test_fill_matches_oracle_fill():
     (dict(stencil="jacobi-2d", n=64, steps=1, T=9, bx=16, by=16), "INVALID_GEOMETRY"),
     (dict(stencil="jacobi-2d", n=64, steps=1, phase_limit=4), "INVALID_ARGUMENT"),
     (dict(stencil="jacobi-2d", n=64, steps=1, engine=7), "INVALID_ARGUMENT"),
-    (dict(stencil="fdtd-2d", n=64, steps=1, impl=3), "INVALID_ARGUMENT"),
+    (dict(stencil="fdtd-2d", n=64, steps=1, impl=2), "INVALID_ARGUMENT"),
 ])
 def test_invalid_parameters_report_status(kw, status):
     with pytest.raises(ots.OtsError) as ei:

@@ -299,18 +299,17 @@ def test_stream2d_packed_kernel_matches_oracle(st, T):
 @pytest.mark.gpu
 @pytest.mark.parametrize("variant", [0, 1])
 @pytest.mark.parametrize("T", [1, 2, 3, 5, 6])
-def test_fdtd_packed_and_scalar_stream_kernels_agree_with_oracle(variant, T):
-    # FDTD-2D's two-phase streamed kernel in packed FP32 (stream_impl 2) and
-    # scalar (0, the default, and 1): bit for bit against the oracle, with the
-    # source row (variant 0) and the reference's +Ey (variant 1), rows not a
-    # multiple of 4
+def test_fdtd_stream_kernel_ragged_widths_and_segments_match_oracle(variant, T):
+    # FDTD-2D's two-phase streamed kernel, bit for bit against the oracle with
+    # the source row (variant 0) and the reference's +Ey (variant 1), rows not
+    # a multiple of 4, in the model's segments and in 8-row ones (iterations
+    # whose level rows all lie inside the grid skip the row test)
     for n in (140, 141, 143):
         outs = []
-        for impl in (2, 0):
-            with ots.Plan("fdtd-2d", n, 2 * T + 1, T=T, bx=32, by=1, E=1, kernel="stream",
-                          variant=variant, impl=impl) as plan:
-                assert plan.describe()["Stream Arithmetic"] == ("packed-fp32" if impl == 2
-                                                                else "scalar")
+        for by in (1, 8):
+            with ots.Plan("fdtd-2d", n, 2 * T + 1, T=T, bx=32, by=by, E=1, kernel="stream",
+                          variant=variant) as plan:
+                assert plan.describe()["Stream Arithmetic"] == "scalar"
                 g = plan.geometry
                 state, aux = inputs(plan, seed=41 + T)
                 plan.upload(state, aux)
